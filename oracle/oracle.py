@@ -1,0 +1,176 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes binding of ``_build/liboracle.so``, the CPU restatement of the SOD2D
+reference arithmetic (``oracle_ops.hpp``).  Imported only by tests/,
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    out = HERE / "_build" / "liboracle.so"
+    if force or not out.exists() or any(
+            (HERE / s).stat().st_mtime > out.stat().st_mtime for s in ("oracle_capi.cpp", "oracle_ops.hpp")):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return out
+
+
+class MeshT(C.Structure):
+    _fields_ = [("porder", C.c_int), ("nelem", C.c_int), ("npoin", C.c_int), ("npoin_w", C.c_int),
+                ("connec", C.c_void_p), ("lpoin_w", C.c_void_p), ("invAtoIJK", C.c_void_p),
+                ("gmshAtoI", C.c_void_p), ("gmshAtoJ", C.c_void_p), ("gmshAtoK", C.c_void_p),
+                ("lelpn", C.c_void_p), ("atoIJK", C.c_void_p),
+                ("He", C.c_void_p), ("gpvol", C.c_void_p), ("dlxigp_ip", C.c_void_p), ("dNgp", C.c_void_p),
+                ("Ngp", C.c_void_p), ("Ml", C.c_void_p), ("invMl", C.c_void_p), ("helem", C.c_void_p),
+                ("helem_l", C.c_void_p), ("volT", C.c_double)]
+
+
+class CompParams(C.Structure):
+    _fields_ = [("gamma", C.c_double), ("Rgas", C.c_double), ("Cp", C.c_double), ("Prt", C.c_double),
+                ("rho_inf", C.c_double), ("p_inf", C.c_double), ("cfl_conv", C.c_double),
+                ("cfl_diff", C.c_double), ("maxPhysTime", C.c_double), ("stages", C.c_int),
+                ("rk_n", C.c_int), ("lps", C.c_int), ("log_first", C.c_int), ("log_step", C.c_int),
+                ("first_mue", C.c_int)]
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(str(build()))
+        for s in ("f32", "f64"):
+            for name in ("tgv_comp_run", "rhs", "entropy_visc", "elem_jacobian", "convec", "comp_tau",
+                         "dt", "analysis"):
+                f = getattr(_lib, f"oracle_{name}_{s}")
+                f.restype = C.c_int
+            getattr(_lib, f"oracle_tgv_comp_run_{s}").argtypes = [
+                C.POINTER(MeshT), C.POINTER(CompParams), C.c_void_p, C.c_double, C.c_int, C.c_void_p,
+                C.c_int, C.POINTER(C.c_int), C.c_void_p]
+            getattr(_lib, f"oracle_rhs_{s}").argtypes = [C.POINTER(MeshT), C.POINTER(CompParams)] + [C.c_void_p] * 10
+            getattr(_lib, f"oracle_entropy_visc_{s}").argtypes = (
+                [C.POINTER(MeshT), C.POINTER(CompParams)] + [C.c_void_p] * 8 + [C.c_double] + [C.c_void_p] * 3)
+            getattr(_lib, f"oracle_elem_jacobian_{s}").argtypes = [C.c_int] * 3 + [C.c_void_p] * 6
+            getattr(_lib, f"oracle_convec_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * 8 + [C.c_int, C.c_double]
+            getattr(_lib, f"oracle_comp_tau_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * 3
+            getattr(_lib, f"oracle_dt_{s}").argtypes = ([C.POINTER(MeshT)] + [C.c_void_p] * 2 + [C.c_double] * 2 +
+                                                        [C.c_void_p] * 5)
+            getattr(_lib, f"oracle_first_mue_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * 6
+            getattr(_lib, f"oracle_first_mue_{s}").restype = C.c_int
+            getattr(_lib, f"oracle_analysis_{s}").argtypes = ([C.POINTER(MeshT), C.c_double] + [C.c_void_p] * 5)
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class OracleMesh:
+    """Holds the oracle's view of a host.Mesh in precision ``dtype``."""
+
+    def __init__(self, mesh, dtype=np.float32, geometry64=None):
+        self.mesh = mesh
+        self.dtype = np.dtype(dtype)
+        self.suffix = "f32" if self.dtype == np.float32 else "f64"
+        cast = lambda a: np.ascontiguousarray(a, dtype=self.dtype)
+        geo = dict(He=mesh.He, gpvol=mesh.gpvol, dlxigp_ip=mesh.dlxigp_ip, dNgp=mesh.dNgp, Ngp=mesh.Ngp,
+                   Ml=mesh.Ml, invMl=mesh.invMl, helem=mesh.helem, helem_l=mesh.helem_l)
+        if geometry64 is not None:
+            geo.update(geometry64)
+        self.arr = {k: cast(v) for k, v in geo.items()}
+        self.ints = {k: np.ascontiguousarray(getattr(mesh, k), np.int32)
+                     for k in ("connecWork", "lpoin_w", "invAtoIJK", "gmshAtoI", "gmshAtoJ", "gmshAtoK",
+                               "lelpn", "atoIJK")}
+        self.volT = float(self.dtype.type(mesh.vol_total if geometry64 is None else geometry64.get(
+            "vol_total", mesh.vol_total)))
+        self.s = MeshT(mesh.porder, mesh.nelem, mesh.npoin, mesh.npoin_w,
+                       _p(self.ints["connecWork"]), _p(self.ints["lpoin_w"]), _p(self.ints["invAtoIJK"]),
+                       _p(self.ints["gmshAtoI"]), _p(self.ints["gmshAtoJ"]), _p(self.ints["gmshAtoK"]),
+                       _p(self.ints["lelpn"]), _p(self.ints["atoIJK"]),
+                       *(_p(self.arr[k]) for k in ("He", "gpvol", "dlxigp_ip", "dNgp", "Ngp", "Ml", "invMl",
+                                                   "helem", "helem_l")), self.volT)
+
+    def fn(self, name):
+        return getattr(lib(), f"oracle_{name}_{self.suffix}")
+
+
+def comp_params(ic, cfl_conv=0.5, cfl_diff=0.5, stages=5, rk_n=1, lps=True, maxPhysTime=0.0,
+                log_first=1, log_step=10, first_mue=True) -> CompParams:
+    return CompParams(ic.gamma, ic.Rgas, ic.Cp, ic.Prt, ic.rho0, ic.P0, cfl_conv, cfl_diff, maxPhysTime,
+                      stages, rk_n, int(lps), log_first, log_step, int(first_mue))
+
+
+def tgv_comp_run(om: OracleMesh, ic, prm: CompParams, nsteps: int, max_rows: int = 4096):
+    """Run the compressible TGV time loop; returns (history[rows,6], final)
+    where history columns are time, EK, eps_S, eps_D, eps_T, max Mach and
+    final = dict(rho, q, E, mu_e)."""
+    N, n = om.mesh.npoin, om.mesh.nnode
+    dt = om.dtype
+    init = np.concatenate([ic.rho, ic.u, ic.q, ic.pr, ic.E, ic.Tem, ic.e_int, ic.csound, ic.machno,
+                           ic.eta]).astype(dt)
+    hist = np.zeros((max_rows, 6))
+    nrows = C.c_int()
+    final = np.zeros(5 * N + om.mesh.nelem * n, dt)
+    rc = om.fn("tgv_comp_run")(C.byref(om.s), C.byref(prm), _p(init), ic.mu_factor, nsteps, _p(hist),
+                               max_rows, C.byref(nrows), _p(final))
+    if rc:
+        raise RuntimeError(f"oracle tgv run failed {rc}")
+    out = dict(rho=final[:N], q=final[N:4 * N], E=final[4 * N:5 * N], mu_e=final[5 * N:])
+    return hist[: nrows.value], out
+
+
+def rhs(om: OracleMesh, prm: CompParams, rho, q, E, mu_e, mu_factor, tau_stab, want_proj=False):
+    """One RHS evaluation (updateF body).  Returns Rmass, Rmom(N*3), Rener
+    (and the 15 mass-inverted projections if want_proj)."""
+    N = om.mesh.npoin
+    dt = om.dtype
+    c = lambda a: np.ascontiguousarray(a, dt)
+    Rm, Rq, Re = np.zeros(N, dt), np.zeros(3 * N, dt), np.zeros(N, dt)
+    proj = np.zeros(15 * N, dt) if want_proj else None
+    mf = np.full(N, mu_factor, dt) if np.isscalar(mu_factor) else c(mu_factor)
+    rc = om.fn("rhs")(C.byref(om.s), C.byref(prm), _p(c(rho)), _p(c(q)), _p(c(E)), _p(c(mu_e)), _p(mf),
+                      _p(c(tau_stab)), _p(Rm), _p(Rq), _p(Re), _p(proj))
+    if rc:
+        raise RuntimeError("oracle rhs failed")
+    return (Rm, Rq, Re, proj) if want_proj else (Rm, Rq, Re)
+
+
+def comp_tau(om: OracleMesh, csound, u):
+    out = np.zeros(om.mesh.nelem, om.dtype)
+    om.fn("comp_tau")(C.byref(om.s), _p(np.ascontiguousarray(csound, om.dtype)),
+                      _p(np.ascontiguousarray(u, om.dtype)), _p(out))
+    return out
+
+
+def first_mue(om: OracleMesh, rho1, u1, eta1, csound):
+    """First-step entropy viscosity and lumped entropy residual."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    mu_e = np.zeros(om.mesh.nelem * om.mesh.nnode, om.dtype)
+    Reta = np.zeros(om.mesh.npoin, om.dtype)
+    om.fn("first_mue")(C.byref(om.s), _p(c(rho1)), _p(c(u1)), _p(c(eta1)), _p(c(csound)), _p(mu_e), _p(Reta))
+    return mu_e, Reta
+
+
+def elem_jacobian(porder, nelem, npoin, connec, coord, dNgp, wgp, dtype=np.float64):
+    dt = np.dtype(dtype)
+    n = (porder + 1) ** 3
+    gpvol = np.zeros(n * nelem, dt)
+    He = np.zeros(9 * n * nelem, dt)
+    s = "f32" if dt == np.float32 else "f64"
+    c = lambda a: np.ascontiguousarray(a, dt)
+    rc = getattr(lib(), f"oracle_elem_jacobian_{s}")(porder, nelem, npoin, _p(np.ascontiguousarray(connec, np.int32)),
+                                                    _p(c(coord)), _p(c(dNgp)), _p(c(wgp)), _p(gpvol), _p(He))
+    if rc:
+        raise RuntimeError("oracle elem_jacobian failed")
+    return gpvol, He
+
+
+def load_history(path) -> np.ndarray:
+    return np.loadtxt(path, ndmin=2)
