@@ -1,0 +1,148 @@
+/*
+ * sod2d_gpu.h -- C-ABI of the B200 (sm_100a) spectral-element RHS library.
+ *
+ * Drop-in for the hot-path subroutines of the SOD2D Fortran solver.  A
+ * Fortran caller binds each function with `interface ... bind(C, name=...)`
+ * (the pattern of src/lib_sod2d/sources/mod_nvtx.f90:27-45) and passes
+ * device addresses with `!$acc host_data use_device(...)`, as
+ * src/lib_sod2d/sources/mod_comms.f90:1083-1092 already does for NCCL.
+ *
+ * Conventions
+ *  - Arrays keep the reference's Fortran layout: column-major, so a field
+ *    X(npoin,3) is three contiguous blocks of npoin values; connectivity
+ *    holds 1-based node ids.  Paths are relative to the reference project.
+ *  - sod_gpu_init() takes HOST pointers and builds the library's own
+ *    device-resident mirrors (element-major connectivity in tensor order,
+ *    packed J^-1 + Gauss weights per element, node->slot CSR for the
+ *    assembly).  Every other call takes DEVICE pointers.
+ *  - All calls are complete on return (the reference's OpenACC regions are
+ *    synchronous), unless sod_gpu_set_stream() selected a stream and
+ *    sod_gpu_set_async(ctx, 1) was called, in which case work is only
+ *    enqueued on that stream.
+ *  - Functions return 0 on success and a negative SOD_GPU_E* code on error;
+ *    sod_gpu_last_error() describes the last failure of the calling thread.
+ *    The Fortran shim turns a non-zero status into `stop 1`.
+ *  - Assembly is deterministic: each element writes its contributions to its
+ *    own slots and a node-centric pass sums them in a fixed order with
+ *    Kahan compensation (no floating-point atomics), so two runs give
+ *    bit-identical results.
+ */
+#ifndef SOD2D_GPU_H
+#define SOD2D_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOD_GPU_OK 0
+#define SOD_GPU_EINVAL -1    /* bad argument or unsupported size          */
+#define SOD_GPU_ECUDA -2     /* a CUDA runtime call failed                */
+#define SOD_GPU_ENOMEM -3    /* device allocation failed                  */
+#define SOD_GPU_ENONFINITE -4 /* a reduction returned NaN/Inf              */
+#define SOD_GPU_ESTAGNATE -5 /* an iterative solve stopped making progress */
+
+typedef struct sod_gpu_ctx sod_gpu_ctx;
+
+/* Mesh and geometry, HOST pointers, reference layout.  Mirrors the arrays
+ * the solver classes hold after CFDSolverBase_evalJacobians / evalMass
+ * (src/lib_mainBaseClass/sources/CFDSolverBase.f90:1638-1795). */
+typedef struct {
+  int porder;            /* element order; 3 and 4 are built             */
+  int nelem, npoin, npoin_w;
+  const int *connec;     /* connecParWork(nelem,nnode), 1-based          */
+  const int *lpoin_w;    /* workingNodesPar(npoin_w), 1-based            */
+  const int *invAtoIJK;  /* invAtoIJK(P+1,P+1,P+1)                       */
+  const int *gmshAtoI, *gmshAtoJ, *gmshAtoK; /* (nnode)                  */
+  const float *dlxigp_ip; /* dlxigp_ip(ngaus,3,P+1)                      */
+  const float *He;       /* He(3,3,ngaus,nelem)                          */
+  const float *gpvol;    /* gpvol(1,ngaus,nelem)                         */
+  const float *Ml;       /* Ml(npoin)                                    */
+  const float *invMl;    /* invMl(npoin)                                 */
+  const float *helem;    /* helem(nelem)       (may be NULL)             */
+  const float *helem_l;  /* helem_l(nelem,nnode) (may be NULL)           */
+  const int *lelpn;      /* lelpn(npoin)       (may be NULL)             */
+} sod_mesh_t;
+
+/* Gas and stabilisation constants of the compressible path
+ * (src/lib_sod2d/sources/mod_numerical_params.f90:27-52, TGVCompSolver.f90:128-146). */
+typedef struct {
+  float gamma_gas, Rgas, Cp, Prt;
+  float c_lps;          /* c_lps_comp = 0.1                                */
+  float c_rho, c_ener;  /* 1, 1                                            */
+  float ce, cmax, cglob;/* ce_comp = 1 (high-Mach path), 0.5, 1            */
+  float ducros_min_val; /* 0.1                                             */
+  float c_species_stab; /* tau scale of comp_tau, 0.5                      */
+  float p_inf, rho_inf; /* nscbc_p_inf, nscbc_rho_inf (entropy scaling)    */
+} sod_phys_t;
+
+/* ---- context --------------------------------------------------------- */
+int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **out);
+int sod_gpu_finalize(sod_gpu_ctx *ctx);
+int sod_gpu_set_stream(sod_gpu_ctx *ctx, void *cuda_stream);
+int sod_gpu_set_async(sod_gpu_ctx *ctx, int async_enabled);
+int sod_gpu_synchronize(sod_gpu_ctx *ctx);
+const char *sod_gpu_last_error(void);
+/* Device bytes held by the context (mirrors + scratch). */
+size_t sod_gpu_device_bytes(const sod_gpu_ctx *ctx);
+
+/* ---- element operators (device pointers, FP32, reference layout) ------ */
+
+/* Split-form convective residual.  Replaces full_convec_ijk,
+ * src/lib_sod2d/sources/elem_convec.f90:227-470 (E is the energy-like
+ * variable the caller convects; updateF passes the enthalpy aux_h). */
+int sod_gpu_full_convec_ijk(sod_gpu_ctx *ctx, const float *u, const float *q, const float *rho,
+                            const float *pr, const float *E, float *Rmass, float *Rmom,
+                            float *Rener, int initialze, float fact);
+
+/* Assembled, lumped-mass-inverted LPS projections.  Replaces full_proj_ijk,
+ * src/lib_sod2d/sources/elem_stab.f90:441-586.  Each Proj* is (npoin,3). */
+int sod_gpu_full_proj_ijk(sod_gpu_ctx *ctx, const float *rho, const float *u, const float *Tem,
+                          float *ProjMass, float *ProjEner, float *ProjMX, float *ProjMY,
+                          float *ProjMZ);
+
+/* Viscous + heat + artificial diffusion with LPS stabilisation.  Replaces
+ * full_diff_stab_ijk, src/lib_sod2d/sources/elem_stab.f90:207-438.
+ * mu_e, mu_sgs are (nelem,ngaus); mu_sgs may be NULL (zero). */
+int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *ctx, float Cp, float Pr, const float *rho_n,
+                               const float *rho, const float *u, const float *Tem,
+                               const float *mu_fluid, const float *mu_e, const float *mu_sgs,
+                               const float *ProjMass, const float *ProjEner, const float *ProjMX,
+                               const float *ProjMY, const float *ProjMZ, const float *tau_stab,
+                               float *Rmass, float *Rmom, float *Rener, int initialze, float fact);
+
+/* R(lpoin_w,:) *= invMl for ncomp components of an (npoin,ncomp) array.
+ * Replaces lumped_solver_scal_opt / lumped_solver_vect_opt,
+ * src/lib_sod2d/sources/mod_solver.f90:41-104. */
+int sod_gpu_lumped_solver(sod_gpu_ctx *ctx, float *R, int ncomp);
+
+/* Store the element viscosity mu_e(nelem,ngaus) in the context (converted
+ * once to the library's element layout).  sod_gpu_updateF called with
+ * mu_e == NULL then uses this copy: the reference keeps mu_e fixed across
+ * the stages of a time step (it is updated once per step, after the
+ * stages, time_integ_ls.f90:455-463). */
+int sod_gpu_set_mu_e(sod_gpu_ctx *ctx, const float *mu_e);
+
+/* One full RHS evaluation from the conserved state (level "pos" arrays):
+ * equation of state, Sutherland viscosity (mu = mu_factor*1.458e-6*
+ * T^1.5/(T+110.4)), convection with E := h, LPS projection, stabilised
+ * diffusion and lumped inversion, fused.  Replaces the body of updateF,
+ * src/lib_sod2d/sources/time_integ_ls.f90:489-691 (periodic, no LES, no
+ * sources).  tau_stab(nelem) comes from sod_gpu_comp_tau; mu_e may be NULL
+ * to use the copy stored by sod_gpu_set_mu_e.  Optional
+ * outputs (NULL to skip): u(npoin,3), pr, Tem, mu_fluid at working nodes. */
+int sod_gpu_updateF(sod_gpu_ctx *ctx, const float *rho, const float *q, const float *E,
+                    const float *mu_e, float mu_factor, const float *tau_stab, float *Rmass,
+                    float *Rmom, float *Rener, float *u_out, float *pr_out, float *Tem_out,
+                    float *mu_fluid_out);
+
+/* tau(nelem) = max_node h_e*(c_species_stab/P)*(c+|u|).  Replaces comp_tau,
+ * src/lib_sod2d/sources/elem_stab.f90:589-616. */
+int sod_gpu_comp_tau(sod_gpu_ctx *ctx, const float *csound, const float *u, float *tau);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

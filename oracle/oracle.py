@@ -142,6 +142,16 @@ def rhs(om: OracleMesh, prm: CompParams, rho, q, E, mu_e, mu_factor, tau_stab, w
     return (Rm, Rq, Re, proj) if want_proj else (Rm, Rq, Re)
 
 
+def convec(om: OracleMesh, u, q, rho, pr, E, init=True, fact=-1.0, R=None):
+    """full_convec_ijk on the oracle (returns Rmass, Rmom(N*3), Rener)."""
+    N = om.mesh.npoin
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    Rm, Rq, Re = (np.zeros(N, om.dtype), np.zeros(3 * N, om.dtype), np.zeros(N, om.dtype)) if R is None else R
+    om.fn("convec")(C.byref(om.s), _p(c(u)), _p(c(q)), _p(c(rho)), _p(c(pr)), _p(c(E)), _p(Rm), _p(Rq), _p(Re),
+                    int(init), float(fact))
+    return Rm, Rq, Re
+
+
 def comp_tau(om: OracleMesh, csound, u):
     out = np.zeros(om.mesh.nelem, om.dtype)
     om.fn("comp_tau")(C.byref(om.s), _p(np.ascontiguousarray(csound, om.dtype)),

@@ -1,0 +1,136 @@
+"""Python view of the C-ABI in ``include/sod2d_gpu.h`` (``libsod2d_gpu.so``).
+
+Device buffers come from torch (plumbing only); every call goes through the
+C entry points with raw device pointers, exactly as a Fortran caller would
+bind them.  Importing this module on a machine without CUDA works; creating
+a ``Context`` needs a GPU and fails loudly if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+P_I = C.POINTER(C.c_int)
+P_F = C.POINTER(C.c_float)
+VP = C.c_void_p
+
+
+class SodMesh(C.Structure):
+    _fields_ = [("porder", C.c_int), ("nelem", C.c_int), ("npoin", C.c_int), ("npoin_w", C.c_int),
+                ("connec", VP), ("lpoin_w", VP), ("invAtoIJK", VP), ("gmshAtoI", VP), ("gmshAtoJ", VP),
+                ("gmshAtoK", VP), ("dlxigp_ip", VP), ("He", VP), ("gpvol", VP), ("Ml", VP), ("invMl", VP),
+                ("helem", VP), ("helem_l", VP), ("lelpn", VP)]
+
+
+class SodPhys(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("gamma_gas", "Rgas", "Cp", "Prt", "c_lps", "c_rho", "c_ener", "ce",
+                                         "cmax", "cglob", "ducros_min_val", "c_species_stab", "p_inf",
+                                         "rho_inf")]
+
+
+# name -> (restype, argtypes); every entry point declared in sod2d_gpu.h
+SIGNATURES = {
+    "sod_gpu_init": (C.c_int, [C.POINTER(SodMesh), C.POINTER(SodPhys), C.POINTER(VP)]),
+    "sod_gpu_finalize": (C.c_int, [VP]),
+    "sod_gpu_set_stream": (C.c_int, [VP, VP]),
+    "sod_gpu_set_async": (C.c_int, [VP, C.c_int]),
+    "sod_gpu_synchronize": (C.c_int, [VP]),
+    "sod_gpu_last_error": (C.c_char_p, []),
+    "sod_gpu_device_bytes": (C.c_size_t, [VP]),
+    "sod_gpu_full_convec_ijk": (C.c_int, [VP] + [VP] * 8 + [C.c_int, C.c_float]),
+    "sod_gpu_full_proj_ijk": (C.c_int, [VP] + [VP] * 8),
+    "sod_gpu_full_diff_stab_ijk": (C.c_int, [VP, C.c_float, C.c_float] + [VP] * 15 + [C.c_int, C.c_float]),
+    "sod_gpu_lumped_solver": (C.c_int, [VP, VP, C.c_int]),
+    "sod_gpu_updateF": (C.c_int, [VP, VP, VP, VP, VP, C.c_float] + [VP] * 8),
+    "sod_gpu_comp_tau": (C.c_int, [VP, VP, VP, VP]),
+    "sod_gpu_set_mu_e": (C.c_int, [VP, VP]),
+}
+
+
+def lib_path():
+    return _build.LIBDIR / "libsod2d_gpu.so"
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not path.exists():
+            raise RuntimeError(f"{path} is missing: run `python -m sod2d_b200.build` (no CPU fallback exists)")
+        _lib = C.CDLL(str(path))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(_lib, name)
+            f.restype = res
+            f.argtypes = args
+    return _lib
+
+
+def check(rc, what=""):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed ({rc}): {lib().sod_gpu_last_error().decode()}")
+
+
+def _hp(a):
+    return None if a is None else a.ctypes.data_as(VP)
+
+
+def dptr(t):
+    """Device pointer of a torch CUDA tensor (None -> NULL)."""
+    return None if t is None else VP(t.data_ptr())
+
+
+def default_phys(gamma=1.4, Rgas=None, Cp=None, Prt=0.71, p_inf=None, rho_inf=1.0, Ma=0.1) -> SodPhys:
+    if Rgas is None:
+        Rgas = 1.0 / (gamma * Ma * Ma)
+    if Cp is None:
+        Cp = gamma * Rgas / (gamma - 1.0)
+    if p_inf is None:
+        p_inf = 1.0 / (gamma * Ma * Ma)
+    return SodPhys(gamma, Rgas, Cp, Prt, np.float32(0.1), 1.0, 1.0, 1.0, 0.5, 1.0, 0.1, 0.5, p_inf, rho_inf)
+
+
+def phys_from_ic(ic) -> SodPhys:
+    return SodPhys(ic.gamma, ic.Rgas, ic.Cp, ic.Prt, np.float32(0.1), 1.0, 1.0, 1.0, 0.5, 1.0, 0.1, 0.5, ic.P0,
+                   ic.rho0)
+
+
+class Context:
+    """Owns a sod_gpu_ctx built from a host.Mesh."""
+
+    def __init__(self, mesh, phys: SodPhys):
+        self.mesh = mesh
+        self._keep = {k: np.ascontiguousarray(getattr(mesh, k)) for k in (
+            "connecWork", "lpoin_w", "invAtoIJK", "gmshAtoI", "gmshAtoJ", "gmshAtoK", "dlxigp_ip", "He", "gpvol",
+            "Ml", "invMl", "helem", "helem_l", "lelpn")}
+        k = self._keep
+        self.sm = SodMesh(mesh.porder, mesh.nelem, mesh.npoin, mesh.npoin_w, _hp(k["connecWork"]), _hp(k["lpoin_w"]),
+                          _hp(k["invAtoIJK"]), _hp(k["gmshAtoI"]), _hp(k["gmshAtoJ"]), _hp(k["gmshAtoK"]),
+                          _hp(k["dlxigp_ip"]), _hp(k["He"]), _hp(k["gpvol"]), _hp(k["Ml"]), _hp(k["invMl"]),
+                          _hp(k["helem"]), _hp(k["helem_l"]), _hp(k["lelpn"]))
+        self.phys = phys
+        h = VP()
+        check(lib().sod_gpu_init(C.byref(self.sm), C.byref(self.phys), C.byref(h)), "sod_gpu_init")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().sod_gpu_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def call(self, name, *args):
+        check(getattr(lib(), name)(self.h, *args), name)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().sod_gpu_device_bytes(self.h))
