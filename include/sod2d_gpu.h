@@ -64,6 +64,7 @@ typedef struct {
   const float *helem;    /* helem(nelem)       (may be NULL)             */
   const float *helem_l;  /* helem_l(nelem,nnode) (may be NULL)           */
   const int *lelpn;      /* lelpn(npoin)       (may be NULL)             */
+  const float *Ngp;      /* Ngp(ngaus,nnode)   (may be NULL: Kronecker)  */
 } sod_mesh_t;
 
 /* Gas and stabilisation constants of the compressible path
@@ -141,6 +142,39 @@ int sod_gpu_updateF(sod_gpu_ctx *ctx, const float *rho, const float *q, const fl
 /* tau(nelem) = max_node h_e*(c_species_stab/P)*(c+|u|).  Replaces comp_tau,
  * src/lib_sod2d/sources/elem_stab.f90:589-616. */
 int sod_gpu_comp_tau(sod_gpu_ctx *ctx, const float *csound, const float *u, float *tau);
+
+/* ---- compressible time integration with library-owned state ----------
+ * The conserved state lives on the device in FP64 (fp64_state = 1) or in
+ * FP32 (fp64_state = 0, the reference's USE_RP=4 arithmetic); the element
+ * kernels always read an FP32 copy.  The step restates rk_4_ls_main,
+ * src/lib_sod2d/sources/time_integ_ls.f90:202-487, for periodic meshes:
+ * first-step entropy viscosity, the low-storage stages (stage 1 reuses the
+ * residual left by the previous step), end-of-step equation of state,
+ * thermodynamic entropy, entropy residual, smart_visc_spectral_imex with
+ * the Ducros limiter, Sutherland viscosity. */
+typedef struct {
+  int stages;      /* 3, 4 (SSPRK(4,3)) or 5 (SSP53_2N)                    */
+  int rk_n;        /* SSP53_2N variant (1..4) when stages == 5             */
+  int fp64_state;  /* 1: FP64 conserved state, 0: FP32                      */
+  float mu_factor; /* Sutherland scale flag_mu_factor                      */
+} sod_rk_cfg_t;
+
+/* Level-2 initial state (device pointers, reference layout): rho, u(N,3),
+ * q(N,3), pr, E, Tem, csound, machno, eta.  mu_e starts at zero. */
+int sod_gpu_comp_init_state(sod_gpu_ctx *ctx, const sod_rk_cfg_t *cfg, const float *rho, const float *u,
+                            const float *q, const float *pr, const float *E, const float *Tem,
+                            const float *csound, const float *machno, const float *eta);
+/* One time step of size dt. */
+int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *ctx, float dt);
+/* CFL time step (adapt_dt_cfl, src/lib_sod2d/sources/mod_time_ops.f90:11-62),
+ * written to *dt (host). */
+int sod_gpu_comp_adapt_dt(sod_gpu_ctx *ctx, float cfl_conv, float cfl_diff, float *dt);
+/* Analysis integrals (mod_analysis.f90:10-168): out[0..4] (host) = EK,
+ * eps_S, eps_D, eps_T, max Mach; FP64 accumulation across elements. */
+int sod_gpu_comp_analysis(sod_gpu_ctx *ctx, float rho0, double *out);
+/* Copies of the current state (device pointers, reference layout; any may
+ * be NULL): rho, q(N,3), E and mu_e(nelem,ngaus). */
+int sod_gpu_comp_get_state(sod_gpu_ctx *ctx, float *rho, float *q, float *E, float *mu_e);
 
 #ifdef __cplusplus
 }

@@ -2,6 +2,7 @@
 // (declarations and contracts: include/sod2d_gpu.h).
 #include "sod2d_gpu.h"
 #include "rhs_kernels.cuh"
+#include "step_kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -47,6 +48,22 @@ struct sod_gpu_ctx {
   float *slotsA = nullptr, *slotsB = nullptr, *proj16 = nullptr, *mue_t = nullptr, *musgs_t = nullptr;
   size_t bytes = 0;
   std::vector<void *> allocs;
+  // analysis / entropy-viscosity support
+  int *is_work = nullptr;
+  float *Ngp_t = nullptr;  // [g][a] tensor order
+  float volT = 0.f;
+  // compressible time-integration state
+  struct Comp {
+    bool ready = false, fp64 = true, first = true;
+    int stages = 5;
+    double lam[7][7], gam[7][7];
+    float mu_factor = 1.f;
+    void *U1[5], *U2[5];  // double or float
+    float *rho32, *q32, *E32, *u1, *u2, *eint, *pr, *csound, *machno, *Tem, *eta1, *eta2, *feta, *Reta1, *Reta2,
+        *aux, *divU, *vort, *mu_fluid, *tau, *Rmass, *Rmom, *Rener, *part;
+    unsigned int *bits;  // [0] min rho, [1] dt, [2] max Mach
+    double *sums;        // [3]
+  } comp;
 
   MeshDev md() const {
     MeshDev m;
@@ -100,6 +117,16 @@ __global__ void k_elem_to_t(long long nelem, int N, const int *__restrict__ a_of
   long long e = idx / N;
   int t = (int)(idx % N);
   dst[idx] = src[e + nelem * a_of_t[t]];
+}
+
+// Internal [e][t] -> reference-layout (nelem, nnode).
+__global__ void k_t_to_elem(long long nelem, int N, const int *__restrict__ a_of_t, const float *__restrict__ src,
+                            float *__restrict__ dst) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nelem * N) return;
+  long long e = idx / N;
+  int t = (int)(idx % N);
+  dst[e + nelem * a_of_t[t]] = src[idx];
 }
 
 // Five Proj arrays (npoin,3) -> node-major [p][16].
@@ -156,6 +183,7 @@ inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 template <int P>
 struct Launch {
+  static constexpr int P_ = P;
   static constexpr int EPB = (Cfg<P>::NT <= 64) ? 2 : 1;
   static constexpr int TPB = EPB * Cfg<P>::NT;
   static unsigned grid(int nelem) { return nblk(nelem, EPB); }
@@ -282,6 +310,22 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
     for (long long e = 0; e < E; ++e)
       for (int a = 0; a < N; ++a) hl[e * N + t_of_a[a]] = mesh->helem_l[e + E * a];
     if ((rc = c->upload(&c->helem_l_t, hl.data(), hl.size()))) { sod_gpu_finalize(c); return rc; }
+  }
+  {
+    std::vector<int> isw((size_t)NP, 0);
+    for (int t = 0; t < mesh->npoin_w; ++t) isw[lw[t]] = 1;
+    std::vector<float> Nt((size_t)N * N, 0.f);
+    for (int g = 0; g < N; ++g)
+      for (int a = 0; a < N; ++a)
+        Nt[(size_t)t_of_a[g] * N + t_of_a[a]] = mesh->Ngp ? mesh->Ngp[g + (long long)N * a] : (g == a ? 1.f : 0.f);
+    double vol = 0.0;
+    for (long long e = 0; e < E; ++e)
+      for (int a = 0; a < N; ++a) vol += (double)mesh->gpvol[a + (long long)N * e];
+    c->volT = (float)vol;
+    if ((rc = c->upload(&c->is_work, isw.data(), isw.size())) || (rc = c->upload(&c->Ngp_t, Nt.data(), Nt.size()))) {
+      sod_gpu_finalize(c);
+      return rc;
+    }
   }
   *out = c;
   return 0;
@@ -427,6 +471,305 @@ int sod_gpu_updateF(sod_gpu_ctx *c, const float *rho, const float *q, const floa
     k_eos_out<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->npoin, c->lpoin_w, c->ph, c->phys.Rgas,
                                                             mu_factor, rho, q, E, u_out, pr_out, Tem_out,
                                                             mu_fluid_out);
+  return c->finish();
+}
+
+}  // extern "C"
+
+// ---- compressible time integration --------------------------------------
+
+namespace {
+
+int rk_coeffs(int S, int n, double lam[7][7], double gam[7][7]) {
+  for (int i = 0; i < 7; ++i)
+    for (int j = 0; j < 7; ++j) { lam[i][j] = 0.0; gam[i][j] = 0.0; }
+  // time_integ_ls.f90:87-167, 1-based indices
+  if (S == 3) {
+    lam[2][1] = 1.0; lam[3][1] = 3.0 / 4.0; lam[3][2] = 1.0 / 4.0; lam[4][1] = 1.0 / 3.0; lam[4][3] = 2.0 / 3.0;
+    gam[2][1] = 1.0; gam[3][2] = 0.25; gam[4][3] = 2.0 / 3.0;
+  } else if (S == 4) {
+    lam[2][1] = 1.0; lam[3][2] = 1.0; lam[4][1] = 2.0 / 3.0; lam[4][3] = 1.0 / 3.0; lam[5][4] = 1.0;
+    gam[2][1] = 0.5; gam[3][2] = 0.5; gam[4][3] = 1.0 / 6.0; gam[5][4] = 0.5;
+  } else if (S == 5) {
+    lam[2][1] = lam[3][2] = lam[4][3] = lam[5][4] = lam[6][5] = 1.0;
+    if (n == 1) {
+      lam[5][1] = 0.571403511494104; lam[5][4] = 0.428596488505896;
+      gam[2][1] = 0.443568244942995; gam[3][2] = 0.291111420073766; gam[4][3] = 0.270612601278217;
+      gam[5][4] = 0.110577759392786; gam[6][5] = 0.458557505351052;
+    } else if (n == 2) {
+      lam[4][1] = 0.682342861037239; lam[4][3] = 0.317657138962761; lam[6][1] = 0.045230974482400;
+      lam[6][5] = 0.954769025517600;
+      gam[2][1] = 0.465388589249323; gam[3][2] = 0.465388589249323; gam[4][3] = 0.124745797313998;
+      gam[5][4] = 0.465388589249323; gam[6][5] = 0.154263303748666;
+    } else if (n == 3) {
+      lam[5][1] = 0.592032910942121; lam[5][4] = 1.0 - lam[5][1];
+      gam[2][1] = 0.266541020678955; gam[3][2] = 0.548560709048532; gam[4][3] = 0.289517014154401;
+      gam[5][4] = 0.086408328057923; gam[6][5] = 0.462943578481813;
+    } else if (n == 4) {
+      lam[4][1] = 0.707858560931430; lam[4][3] = 1.0 - lam[4][1]; lam[6][1] = 0.222853615080669;
+      lam[6][5] = 1.0 - lam[6][1];
+      gam[2][1] = 0.292845746913355; gam[3][2] = 0.339532793976408; gam[4][3] = 0.200532330324672;
+      gam[5][4] = 0.701676169006879; gam[6][5] = 0.155278812461877;
+    } else {
+      return -1;
+    }
+  } else {
+    return -1;
+  }
+  return 0;
+}
+
+// The FP32 reference rounds its RK coefficients to real(rp): mirror that.
+inline double as_rp(double v, bool fp64) { return fp64 ? v : (double)(float)v; }
+
+template <class T>
+void launch_stage(sod_gpu_ctx *c, double l1, double li, double gdt, int first) {
+  auto &S = c->comp;
+  State5<T> U1, U2;
+  for (int f = 0; f < 5; ++f) { U1.f[f] = (T *)S.U1[f]; U2.f[f] = (T *)S.U2[f]; }
+  k_stage<T><<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->npoin, c->lpoin_w, U1, U2, S.Rmass,
+                                                           S.Rmom, S.Rener, (T)l1, (T)li, (T)gdt, first, S.rho32,
+                                                           S.q32, S.E32);
+}
+
+// RHS at the current FP32 shadow state into comp.R* (updateF body).
+void comp_updateF(sod_gpu_ctx *c) {
+  auto &S = c->comp;
+  RhsArgs A{};
+  A.rho = S.rho32; A.q = S.q32; A.E = S.E32; A.mu_factor = S.mu_factor;
+  A.mue_t = c->mue_t; A.tau_stab = S.tau; A.proj16 = c->proj16;
+  A.fact_c = -1.0f; A.fact_d = -1.0f;
+  dispatch(c, [&](auto L) {
+    L.proj(c, false, S.rho32, S.q32, S.E32);
+    gather_proj_aos(c);
+    L.template rhs<MODE_CONV | MODE_DIFF, IN_CONS>(c, A);
+    return 0;
+  });
+  gather_res(c, S.Rmass, S.Rmom, S.Rener, 0, 1);
+}
+
+// Entropy residual (+ divergence and vorticity when dc) of (feta, eta1, u1[, u2]).
+void comp_entropy_pass(sod_gpu_ctx *c, float *Reta_out, bool dc) {
+  auto &S = c->comp;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    constexpr int P = LL::P_;
+    if (dc)
+      k_entropy_elem<P, LL::EPB, true><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), S.feta, S.eta1, S.u1,
+                                                                                     S.u2, c->slotsB);
+    else
+      k_entropy_elem<P, LL::EPB, false><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), S.feta, S.eta1, S.u1,
+                                                                                      S.u2, c->slotsB);
+    return 0;
+  });
+  k_gather_entropy<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, c->lelpn, c->is_work, Reta_out,
+                                                               S.divU, S.vort, dc ? 1 : 0);
+}
+
+void comp_visc(sod_gpu_ctx *c, const float *Reta, const float *rho, const float *u, bool ducros) {
+  auto &S = c->comp;
+  const unsigned init_bits = 0x47C35000u;  // 100000.0f
+  cudaMemcpyAsync(S.bits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream);
+  k_min_rho<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, S.bits);
+  ViscArgs V{};
+  V.Reta = Reta; V.rho = rho; V.u = u; V.csound = S.csound; V.divU = S.divU; V.vort = S.vort; V.Ml = c->Ml;
+  V.helem = c->helem; V.helem_l_t = c->helem_l_t; V.min_rho_bits = S.bits;
+  V.ce = c->phys.ce; V.cmax = c->phys.cmax; V.cglob = c->phys.cglob; V.ducros_min = c->phys.ducros_min_val;
+  V.inv_p = 1.0f / (float)c->P; V.ducros = ducros ? 1 : 0;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_visc<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), V, c->a_of_t, c->mue_t, nullptr);
+    return 0;
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int sod_gpu_comp_init_state(sod_gpu_ctx *c, const sod_rk_cfg_t *cfg, const float *rho, const float *u,
+                            const float *q, const float *pr, const float *E, const float *Tem, const float *csound,
+                            const float *machno, const float *eta) {
+  if (!c || !cfg || !rho || !u || !q || !pr || !E || !Tem || !csound || !machno || !eta)
+    return fail(SOD_GPU_EINVAL, "bad argument");
+  if (!c->helem || !c->helem_l_t || !c->lelpn) return fail(SOD_GPU_EINVAL, "time integration needs helem, helem_l and lelpn at init");
+  auto &S = c->comp;
+  if (rk_coeffs(cfg->stages, cfg->rk_n, S.lam, S.gam)) return fail(SOD_GPU_EINVAL, "unsupported RK scheme");
+  const size_t N = c->npoin, NE = (size_t)c->nelem;
+  int rc = 0;
+  if (!S.ready) {
+    const size_t tb = cfg->fp64_state ? sizeof(double) : sizeof(float);
+    for (int f = 0; f < 5; ++f) {
+      char *p1, *p2;
+      if ((rc = c->alloc(&p1, N * tb)) || (rc = c->alloc(&p2, N * tb))) return rc;
+      S.U1[f] = p1; S.U2[f] = p2;
+    }
+    float **f1[] = {&S.rho32, &S.E32, &S.eint, &S.pr, &S.csound, &S.machno, &S.Tem, &S.eta1, &S.eta2,
+                    &S.Reta1, &S.Reta2, &S.aux, &S.divU, &S.mu_fluid, &S.Rmass, &S.Rener};
+    for (auto pp : f1)
+      if ((rc = c->alloc(pp, N))) return rc;
+    float **f3[] = {&S.q32, &S.u1, &S.u2, &S.feta, &S.vort, &S.Rmom};
+    for (auto pp : f3)
+      if ((rc = c->alloc(pp, 3 * N))) return rc;
+    if ((rc = c->alloc(&S.tau, NE)) || (rc = c->alloc(&S.part, 3 * NE)) || (rc = c->alloc(&S.bits, 4)) ||
+        (rc = c->alloc(&S.sums, 4)))
+      return rc;
+    S.ready = true;
+    S.fp64 = cfg->fp64_state != 0;
+  } else if ((cfg->fp64_state != 0) != S.fp64) {
+    return fail(SOD_GPU_EINVAL, "state precision cannot change after the first init");
+  }
+  S.stages = cfg->stages;
+  S.mu_factor = cfg->mu_factor;
+  S.first = true;
+  const cudaStream_t st = c->stream;
+  CUDA_TRY(cudaMemcpyAsync(S.rho32, rho, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.q32, q, 3 * N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.E32, E, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.u2, u, 3 * N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.pr, pr, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.Tem, Tem, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.csound, csound, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.machno, machno, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.eta2, eta, N * 4, cudaMemcpyDeviceToDevice, st));
+  for (float *z : {S.Reta1, S.Reta2, S.Rmass, S.Rener, S.divU, S.aux})
+    CUDA_TRY(cudaMemsetAsync(z, 0, N * 4, st));
+  CUDA_TRY(cudaMemsetAsync(S.Rmom, 0, 3 * N * 4, st));
+  CUDA_TRY(cudaMemsetAsync(S.vort, 0, 3 * N * 4, st));
+  CUDA_TRY(cudaMemsetAsync(c->mue_t, 0, NE * c->N * 4, st));
+  c->mue_set = true;
+  // FP64 (or FP32) master state from the FP32 initial arrays
+  {
+    const float *src[5] = {rho, q, q + N, q + 2 * N, E};
+    std::vector<float> h(N);
+    for (int f = 0; f < 5; ++f) {
+      CUDA_TRY(cudaMemcpyAsync(h.data(), src[f], N * 4, cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+      if (S.fp64) {
+        std::vector<double> d(h.begin(), h.end());
+        CUDA_TRY(cudaMemcpy(S.U2[f], d.data(), N * 8, cudaMemcpyHostToDevice));
+      } else {
+        CUDA_TRY(cudaMemcpy(S.U2[f], h.data(), N * 4, cudaMemcpyHostToDevice));
+      }
+    }
+  }
+  k_sutherland<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->lpoin_w, S.mu_factor, S.Tem, S.mu_fluid);
+  return c->finish();
+}
+
+int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *c, float dt) {
+  if (!c || !c->comp.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
+  if (!(dt > 0.f)) return fail(SOD_GPU_EINVAL, "dt must be positive");
+  auto &S = c->comp;
+  const cudaStream_t st = c->stream;
+  const size_t N = c->npoin;
+  const size_t tb = S.fp64 ? 8 : 4;
+  // level 1 <- level 2 (CFDSolverBase.f90:1951-1960)
+  for (int f = 0; f < 5; ++f) CUDA_TRY(cudaMemcpyAsync(S.U1[f], S.U2[f], N * tb, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.u1, S.u2, 3 * N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.eta1, S.eta2, N * 4, cudaMemcpyDeviceToDevice, st));
+  // tau from level 2 (comp_tau)
+  k_comp_tau<<<nblk(c->nelem, 8), 256, 0, st>>>(c->nelem, c->N, c->conn, c->helem, S.csound, S.u2, c->npoin,
+                                                c->phys.c_species_stab / (float)c->P, S.tau);
+  if (S.first) {
+    S.first = false;
+    k_feta<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->npoin, c->lpoin_w, S.u1, S.eta1, S.feta);
+    comp_entropy_pass(c, S.Reta1, false);
+    comp_visc(c, S.Reta1, S.rho32, S.u1, false);
+    comp_updateF(c);
+  }
+  const double dtd = (double)dt;
+  auto stage = [&](double l1, double li, double g, int first) {
+    const double gdt = S.fp64 ? g * dtd : (double)((float)g * dt);
+    if (S.fp64)
+      launch_stage<double>(c, l1, li, gdt, first);
+    else
+      launch_stage<float>(c, as_rp(l1, false), as_rp(li, false), gdt, first);
+  };
+  stage(0.0, 0.0, as_rp(S.gam[2][1], S.fp64), 1);
+  for (int i = 2; i <= S.stages; ++i) {
+    comp_updateF(c);
+    stage(as_rp(S.lam[i + 1][1], S.fp64), as_rp(S.lam[i + 1][i], S.fp64), as_rp(S.gam[i + 1][i], S.fp64), 0);
+  }
+  const float gm = c->phys.gamma_gas;
+  k_eos_end<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->npoin, c->lpoin_w, gm - 1.0f, gm, c->phys.Rgas,
+                                                   S.rho32, S.q32, S.E32, S.u2, S.eint, S.pr, S.csound, S.machno,
+                                                   S.Tem);
+  k_thermo_entropy<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->npoin, c->lpoin_w, gm, c->phys.p_inf,
+                                                          c->phys.rho_inf, S.rho32, S.pr, S.u1, S.eta1, S.eta2,
+                                                          S.feta);
+  comp_entropy_pass(c, S.Reta2, true);
+  k_aux_reta<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->lpoin_w, dt, S.Reta1, S.Reta2, S.eta1, S.eta2,
+                                                    S.aux);
+  comp_visc(c, S.aux, S.rho32, S.u2, true);
+  k_sutherland<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->lpoin_w, S.mu_factor, S.Tem, S.mu_fluid);
+  return c->finish();
+}
+
+int sod_gpu_comp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float cfl_diff, float *dt) {
+  if (!c || !c->comp.ready || !dt) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &S = c->comp;
+  const unsigned init_bits = 0x56B5E621u;  // 1e14f
+  CUDA_TRY(cudaMemcpyAsync(S.bits + 1, &init_bits, 4, cudaMemcpyHostToDevice, c->stream));
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_dt<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), c->helem, S.u2, S.csound, S.mu_fluid,
+                                                            c->mue_t, S.rho32, cfl_conv, cfl_diff, S.bits + 1);
+    return 0;
+  });
+  unsigned b = 0;
+  CUDA_TRY(cudaMemcpyAsync(&b, S.bits + 1, 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  float v;
+  std::memcpy(&v, &b, 4);
+  *dt = v;
+  return 0;
+}
+
+int sod_gpu_comp_analysis(sod_gpu_ctx *c, float rho0, double *out) {
+  if (!c || !c->comp.ready || !out) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &S = c->comp;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_analysis_elem<LL::P_, LL::EPB><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(
+        c->md(), S.rho32, S.u2, S.mu_fluid, c->mue_t, c->Ngp_t, S.part);
+    return 0;
+  });
+  k_sum_parts<<<1, 1024, 0, c->stream>>>(c->nelem, S.part, S.sums);
+  const unsigned zero = 0u;
+  CUDA_TRY(cudaMemcpyAsync(S.bits + 2, &zero, 4, cudaMemcpyHostToDevice, c->stream));
+  k_max_mach<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, S.machno, S.bits + 2);
+  double sums[3];
+  unsigned mb = 0;
+  CUDA_TRY(cudaMemcpyAsync(sums, S.sums, 24, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(&mb, S.bits + 2, 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const float twopi = 2.0f * 3.14159f;
+  double EK = sums[0] / (double)(rho0 * powf(twopi, 3.0f));
+  const float alpha = 1.0f / (rho0 * c->volT);
+  double eS = sums[1] * (double)alpha;
+  double eD = (double)(4.0f / 3.0f) * sums[2] * (double)alpha;
+  float mach;
+  std::memcpy(&mach, &mb, 4);
+  out[0] = (double)(float)EK;
+  out[1] = (double)(float)eS;
+  out[2] = (double)(float)eD;
+  out[3] = (double)(float)(eS + eD);
+  out[4] = (double)mach;
+  return 0;
+}
+
+int sod_gpu_comp_get_state(sod_gpu_ctx *c, float *rho, float *q, float *E, float *mu_e) {
+  if (!c || !c->comp.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
+  auto &S = c->comp;
+  const size_t N = c->npoin;
+  if (rho) CUDA_TRY(cudaMemcpyAsync(rho, S.rho32, N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  if (q) CUDA_TRY(cudaMemcpyAsync(q, S.q32, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  if (E) CUDA_TRY(cudaMemcpyAsync(E, S.E32, N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  if (mu_e) {
+    const long long EN = (long long)c->nelem * c->N;
+    k_t_to_elem<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, c->mue_t, mu_e);
+  }
   return c->finish();
 }
 

@@ -24,7 +24,11 @@ class SodMesh(C.Structure):
     _fields_ = [("porder", C.c_int), ("nelem", C.c_int), ("npoin", C.c_int), ("npoin_w", C.c_int),
                 ("connec", VP), ("lpoin_w", VP), ("invAtoIJK", VP), ("gmshAtoI", VP), ("gmshAtoJ", VP),
                 ("gmshAtoK", VP), ("dlxigp_ip", VP), ("He", VP), ("gpvol", VP), ("Ml", VP), ("invMl", VP),
-                ("helem", VP), ("helem_l", VP), ("lelpn", VP)]
+                ("helem", VP), ("helem_l", VP), ("lelpn", VP), ("Ngp", VP)]
+
+
+class RkCfg(C.Structure):
+    _fields_ = [("stages", C.c_int), ("rk_n", C.c_int), ("fp64_state", C.c_int), ("mu_factor", C.c_float)]
 
 
 class SodPhys(C.Structure):
@@ -49,6 +53,11 @@ SIGNATURES = {
     "sod_gpu_updateF": (C.c_int, [VP, VP, VP, VP, VP, C.c_float] + [VP] * 8),
     "sod_gpu_comp_tau": (C.c_int, [VP, VP, VP, VP]),
     "sod_gpu_set_mu_e": (C.c_int, [VP, VP]),
+    "sod_gpu_comp_init_state": (C.c_int, [VP, C.POINTER(RkCfg)] + [VP] * 9),
+    "sod_gpu_comp_rk_ls_step": (C.c_int, [VP, C.c_float]),
+    "sod_gpu_comp_adapt_dt": (C.c_int, [VP, C.c_float, C.c_float, C.POINTER(C.c_float)]),
+    "sod_gpu_comp_analysis": (C.c_int, [VP, C.c_float, C.POINTER(C.c_double)]),
+    "sod_gpu_comp_get_state": (C.c_int, [VP] + [VP] * 4),
 }
 
 
@@ -106,12 +115,12 @@ class Context:
         self.mesh = mesh
         self._keep = {k: np.ascontiguousarray(getattr(mesh, k)) for k in (
             "connecWork", "lpoin_w", "invAtoIJK", "gmshAtoI", "gmshAtoJ", "gmshAtoK", "dlxigp_ip", "He", "gpvol",
-            "Ml", "invMl", "helem", "helem_l", "lelpn")}
+            "Ml", "invMl", "helem", "helem_l", "lelpn", "Ngp")}
         k = self._keep
         self.sm = SodMesh(mesh.porder, mesh.nelem, mesh.npoin, mesh.npoin_w, _hp(k["connecWork"]), _hp(k["lpoin_w"]),
                           _hp(k["invAtoIJK"]), _hp(k["gmshAtoI"]), _hp(k["gmshAtoJ"]), _hp(k["gmshAtoK"]),
                           _hp(k["dlxigp_ip"]), _hp(k["He"]), _hp(k["gpvol"]), _hp(k["Ml"]), _hp(k["invMl"]),
-                          _hp(k["helem"]), _hp(k["helem_l"]), _hp(k["lelpn"]))
+                          _hp(k["helem"]), _hp(k["helem_l"]), _hp(k["lelpn"]), _hp(k["Ngp"]))
         self.phys = phys
         h = VP()
         check(lib().sod_gpu_init(C.byref(self.sm), C.byref(self.phys), C.byref(h)), "sod_gpu_init")
