@@ -143,6 +143,56 @@ int sod_gpu_updateF(sod_gpu_ctx *ctx, const float *rho, const float *q, const fl
  * src/lib_sod2d/sources/elem_stab.f90:589-616. */
 int sod_gpu_comp_tau(sod_gpu_ctx *ctx, const float *csound, const float *u, float *tau);
 
+/* ---- incompressible operators (device pointers, FP32, reference layout) */
+
+/* ResP = sum_e int grad N . grad p (assembled, no mass inversion).
+ * Replaces eval_laplacian_mult, src/lib_sod2d_incomp/sources/mod_operators.f90:16-112. */
+int sod_gpu_eval_laplacian_mult(sod_gpu_ctx *ctx, const float *p, float *ResP);
+/* The same operator in FP64 arithmetic on FP64 vectors (FP32 geometry). */
+int sod_gpu_eval_laplacian_mult64(sod_gpu_ctx *ctx, const double *p, double *ResP);
+/* d = sum gpvol |grad N_a|^2.  Replaces eval_laplacian_diag, mod_operators.f90:638-682. */
+int sod_gpu_eval_laplacian_diag(sod_gpu_ctx *ctx, float *d);
+/* Lumped gradient gradX(npoin,3).  Replaces eval_gradient(..., lump=.true.),
+ * mod_operators.f90:212-288. */
+int sod_gpu_eval_gradient(sod_gpu_ctx *ctx, const float *x, float *gradX);
+/* Assembled int N div u.  Replaces eval_divergence, mod_operators.f90:485-570. */
+int sod_gpu_eval_divergence(sod_gpu_ctx *ctx, const float *u, float *divU);
+/* Skew-symmetric momentum convection.  Replaces full_convec_ijk_incomp,
+ * src/lib_sod2d_incomp/sources/elem_convec_incomp.f90:19-125 (Rmom zeroed). */
+int sod_gpu_full_convec_ijk_incomp(sod_gpu_ctx *ctx, const float *u, const float *q, float *Rmom);
+
+/* Jacobi-preconditioned CG for the pressure Poisson problem in the
+ * reference's arithmetic: FP32 vectors, FP64 dot products and norms,
+ * alpha and beta rounded to FP32, Polak-Ribiere beta, x0 = Rp0, stop when
+ * ||r|| < tol ||b|| or after maxIter.  On return R = x0 + x.  Replaces
+ * conjGrad_pressure_incomp, src/lib_sod2d_incomp/sources/mod_solver_incomp.f90:253-506.
+ * *iters and *res_rel (host, may be NULL) receive the iteration count and
+ * ||r||/||b||. */
+int sod_gpu_conjgrad_pressure(sod_gpu_ctx *ctx, const float *Rp0, float *R, int maxIter, double tol,
+                              int *iters, double *res_rel);
+
+/* Pressure solve to an FP64-certified tolerance: flexible CG on FP64
+ * vectors with the FP64 Laplacian; preconditioner 0 = Jacobi, 1 = the
+ * learned element-patch network (sod_gpu_precond_*), falling back to
+ * Jacobi when the residual stagnates.  b is made mean-free over working
+ * nodes (the periodic Laplacian's null space).  Convergence is declared
+ * only when the true residual ||b - A x|| / ||b||, recomputed in FP64,
+ * is below tol. */
+typedef struct {
+  int max_iter;
+  double tol;
+  int precond;         /* 0 Jacobi, 1 learned                                */
+  int stagnation_window; /* iterations without a 2x residual drop -> fallback */
+} sod_solve_opts_t;
+typedef struct {
+  int iterations;
+  int fallback;        /* 1 if the learned preconditioner was abandoned       */
+  double res_rel;      /* true FP64 relative residual at exit                 */
+  double seconds;      /* device time of the solve                            */
+} sod_solve_stats_t;
+int sod_gpu_pressure_solve(sod_gpu_ctx *ctx, const double *b, double *x, const sod_solve_opts_t *opts,
+                           sod_solve_stats_t *stats);
+
 /* ---- compressible time integration with library-owned state ----------
  * The conserved state lives on the device in FP64 (fp64_state = 1) or in
  * FP32 (fp64_state = 0, the reference's USE_RP=4 arithmetic); the element

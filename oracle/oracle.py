@@ -64,6 +64,13 @@ def lib() -> C.CDLL:
                                                         [C.c_void_p] * 5)
             getattr(_lib, f"oracle_first_mue_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * 6
             getattr(_lib, f"oracle_first_mue_{s}").restype = C.c_int
+            for nm, na in (("laplacian", 2), ("laplacian_diag", 1), ("gradient", 2), ("divergence", 2),
+                           ("convec_incomp", 3)):
+                getattr(_lib, f"oracle_{nm}_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * na
+                getattr(_lib, f"oracle_{nm}_{s}").restype = C.c_int
+            getattr(_lib, f"oracle_cg_pressure_{s}").argtypes = ([C.POINTER(MeshT)] + [C.c_void_p] * 3 +
+                                                                 [C.c_int, C.c_double, C.c_void_p, C.c_void_p])
+            getattr(_lib, f"oracle_cg_pressure_{s}").restype = C.c_int
             getattr(_lib, f"oracle_analysis_{s}").argtypes = ([C.POINTER(MeshT), C.c_double] + [C.c_void_p] * 5)
     return _lib
 
@@ -150,6 +157,47 @@ def convec(om: OracleMesh, u, q, rho, pr, E, init=True, fact=-1.0, R=None):
     om.fn("convec")(C.byref(om.s), _p(c(u)), _p(c(q)), _p(c(rho)), _p(c(pr)), _p(c(E)), _p(Rm), _p(Rq), _p(Re),
                     int(init), float(fact))
     return Rm, Rq, Re
+
+
+def _op(om, name, ncomp_out, *inputs):
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = np.zeros(ncomp_out * om.mesh.npoin, om.dtype)
+    keep = [c(a) for a in inputs]
+    om.fn(name)(C.byref(om.s), *(_p(a) for a in keep), _p(out))
+    return out
+
+
+def laplacian(om, p):
+    """eval_laplacian_mult (assembled, not mass-inverted)."""
+    return _op(om, "laplacian", 1, p)
+
+
+def laplacian_diag(om):
+    return _op(om, "laplacian_diag", 1)
+
+
+def gradient(om, x):
+    """eval_gradient with lumped inversion: (N,3)."""
+    return _op(om, "gradient", 3, x)
+
+
+def divergence(om, u):
+    """eval_divergence (assembled int N div u)."""
+    return _op(om, "divergence", 1, u)
+
+
+def convec_incomp(om, u, q):
+    return _op(om, "convec_incomp", 3, u, q)
+
+
+def cg_pressure(om, diag, x0, rhs, maxIter=20, tol=1e-2):
+    """conjGrad_pressure_incomp: returns (x0 + x, iterations, ||r||/||b||)."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = np.zeros(om.mesh.npoin, om.dtype)
+    res = C.c_double()
+    keep = [c(diag), c(x0), c(rhs)]
+    it = om.fn("cg_pressure")(C.byref(om.s), *(_p(a) for a in keep), maxIter, tol, _p(out), C.byref(res))
+    return out, it, res.value
 
 
 def comp_tau(om: OracleMesh, csound, u):

@@ -475,4 +475,43 @@ ORACLE_BOTH(DEF_RUN)
   }
 ORACLE_BOTH(DEF_FIRST)
 
+#define DEF_INCOMP(R, S)                                                                               \
+  int oracle_laplacian_##S(const oracle_mesh_t *cm, const R *p, R *out) {                              \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    eval_laplacian_mult<R>(m, g, p, out);                                                              \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_laplacian_diag_##S(const oracle_mesh_t *cm, R *out) {                                     \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    eval_laplacian_diag<R>(m, g, out);                                                                 \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_gradient_##S(const oracle_mesh_t *cm, const R *x, R *out) {                               \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    eval_gradient<R>(m, g, x, out);                                                                    \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_divergence_##S(const oracle_mesh_t *cm, const R *u, R *out) {                             \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    eval_divergence<R>(m, g, u, out);                                                                  \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_convec_incomp_##S(const oracle_mesh_t *cm, const R *u, const R *q, R *out) {              \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    full_convec_ijk_incomp<R>(m, g, u, q, out);                                                        \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_cg_pressure_##S(const oracle_mesh_t *cm, const R *diag, const R *x0, const R *rhs,        \
+                             int maxIter, double tol, R *out, double *res) {                           \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    return conjGrad_pressure<R>(m, g, diag, x0, rhs, maxIter, tol, out, res);                          \
+  }
+ORACLE_BOTH(DEF_INCOMP)
+
 }  // extern "C"

@@ -767,4 +767,185 @@ void visc_dissipationRate(const Mesh &m, const Geo<R> &g, R rho0, const R *mu_fl
   *eps_D = (double)(R)D;
 }
 
+
+// ---- eval_laplacian_mult, src/lib_sod2d_incomp/sources/mod_operators.f90:16-112
+// ResP = sum_e int grad N . grad p (no fixed-pressure node: periodic TGV).
+template <class R>
+void eval_laplacian_mult(const Mesh &m, const Geo<R> &g, const R *p, R *ResP) {
+  const long long N = m.npoin;
+  const int n = m.nnode;
+  for (long long i = 0; i < N; ++i) ResP[i] = 0;
+  std::vector<R> buf((size_t)m.nelem * n);
+  Idx ix(m);
+#pragma omp parallel for schedule(static)
+  for (long long e = 0; e < m.nelem; ++e) {
+    std::vector<R> pl(n), gP(n * 3);
+    for (int a = 0; a < n; ++a) pl[a] = p[ix.node(e, a)];
+    for (int gp = 0; gp < n; ++gp) {
+      int I = m.gI[gp] - 1, J = m.gJ[gp] - 1, K = m.gK[gp] - 1;
+      R gi[3] = {0, 0, 0};
+      for (int ii = 0; ii < m.np1; ++ii) {
+        gi[0] = gi[0] + DL(g, m, gp, 0, ii) * pl[ix.inv(ii, J, K)];
+        gi[1] = gi[1] + DL(g, m, gp, 1, ii) * pl[ix.inv(I, ii, K)];
+        gi[2] = gi[2] + DL(g, m, gp, 2, ii) * pl[ix.inv(I, J, ii)];
+      }
+      for (int i = 0; i < 3; ++i) {
+        R s = 0;
+        for (int j = 0; j < 3; ++j) s = s + HE(g, m, i, j, gp, e) * gi[j];
+        gP[gp * 3 + i] = s;
+      }
+    }
+    for (int gp = 0; gp < n; ++gp) buf[(size_t)e * n + gp] = weak_div(m, g, ix, e, gp, gP.data());
+  }
+  R *dst[1] = {ResP};
+  scatter(m, buf, 1, dst, R(1));
+}
+
+// ---- eval_laplacian_diag, mod_operators.f90:638-682 ----------------------
+template <class R>
+void eval_laplacian_diag(const Mesh &m, const Geo<R> &g, R *d) {
+  const long long N = m.npoin;
+  const int n = m.nnode;
+  for (long long i = 0; i < N; ++i) d[i] = 0;
+  Idx ix(m);
+  std::vector<R> gpcar(3 * n);
+  for (long long e = 0; e < m.nelem; ++e)
+    for (int gp = 0; gp < n; ++gp) {
+      for (int i = 0; i < 3; ++i)
+        for (int a = 0; a < n; ++a) {
+          R s = 0;
+          for (int j = 0; j < 3; ++j) s = s + HE(g, m, i, j, gp, e) * g.dNgp[j + 3 * (a + n * gp)];
+          gpcar[i + 3 * a] = s;
+        }
+      for (int i = 0; i < 3; ++i)
+        for (int a = 0; a < n; ++a) {
+          int p = ix.node(e, a);
+          d[p] = d[p] + GV(g, m, gp, e) * gpcar[i + 3 * a] * gpcar[i + 3 * a];
+        }
+    }
+}
+
+// ---- eval_gradient (lumped), mod_operators.f90:212-288 --------------------
+template <class R>
+void eval_gradient(const Mesh &m, const Geo<R> &g, const R *x, R *gradX) {
+  const long long N = m.npoin;
+  const int n = m.nnode;
+  for (long long i = 0; i < 3 * N; ++i) gradX[i] = 0;
+  std::vector<R> buf((size_t)m.nelem * n * 3);
+  Idx ix(m);
+#pragma omp parallel for schedule(static)
+  for (long long e = 0; e < m.nelem; ++e) {
+    std::vector<R> pl(n);
+    for (int a = 0; a < n; ++a) pl[a] = x[ix.node(e, a)];
+    for (int gp = 0; gp < n; ++gp) {
+      int I = m.gI[gp] - 1, J = m.gJ[gp] - 1, K = m.gK[gp] - 1;
+      R gi[3] = {0, 0, 0};
+      for (int ii = 0; ii < m.np1; ++ii) {
+        gi[0] = gi[0] + DL(g, m, gp, 0, ii) * pl[ix.inv(ii, J, K)];
+        gi[1] = gi[1] + DL(g, m, gp, 1, ii) * pl[ix.inv(I, ii, K)];
+        gi[2] = gi[2] + DL(g, m, gp, 2, ii) * pl[ix.inv(I, J, ii)];
+      }
+      for (int i = 0; i < 3; ++i) {
+        R s = 0;
+        for (int j = 0; j < 3; ++j) s = s + HE(g, m, i, j, gp, e) * gi[j];
+        buf[((size_t)e * n + gp) * 3 + i] = GV(g, m, gp, e) * s;
+      }
+    }
+  }
+  R *dst[3] = {gradX, gradX + N, gradX + 2 * N};
+  scatter(m, buf, 3, dst, R(1));
+  lumped_solver(m, g, gradX, 3);
+}
+
+// ---- full_convec_ijk_incomp, src/lib_sod2d_incomp/sources/elem_convec_incomp.f90:19-125
+template <class R>
+void full_convec_ijk_incomp(const Mesh &m, const Geo<R> &g, const R *u, const R *q, R *Rmom) {
+  const long long N = m.npoin;
+  const int n = m.nnode;
+  for (long long i = 0; i < 3 * N; ++i) Rmom[i] = 0;
+  std::vector<R> buf((size_t)m.nelem * n * 3);
+  Idx ix(m);
+#pragma omp parallel for schedule(static)
+  for (long long e = 0; e < m.nelem; ++e) {
+    std::vector<R> ul(n * 3), ql(n * 3);
+    for (int a = 0; a < n; ++a) {
+      int p = ix.node(e, a);
+      for (int d = 0; d < 3; ++d) { ul[a * 3 + d] = u[p + N * d]; ql[a * 3 + d] = q[p + N * d]; }
+    }
+    for (int gp = 0; gp < n; ++gp) {
+      int I = m.gI[gp] - 1, J = m.gJ[gp] - 1, K = m.gK[gp] - 1;
+      R gQ[3][3] = {}, gF[3][3][3] = {};
+      for (int ii = 0; ii < m.np1; ++ii) {
+        int an[3] = {ix.inv(ii, J, K), ix.inv(I, ii, K), ix.inv(I, J, ii)};
+        for (int i = 0; i < 3; ++i) {
+          for (int d = 0; d < 3; ++d) gQ[i][d] = gQ[i][d] + DL(g, m, gp, d, ii) * ql[an[d] * 3 + i];
+          for (int j = 0; j < 3; ++j)
+            for (int d = 0; d < 3; ++d)
+              gF[i][j][d] = gF[i][j][d] + DL(g, m, gp, d, ii) * ql[an[d] * 3 + i] * ul[an[d] * 3 + j];
+        }
+      }
+      R gradQ[3][3] = {}, divF[3] = {0, 0, 0};
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          for (int k = 0; k < 3; ++k) {
+            gradQ[i][j] = gradQ[i][j] + HE(g, m, j, k, gp, e) * gQ[i][k];
+            divF[i] = divF[i] + HE(g, m, j, k, gp, e) * gF[i][j][k];
+          }
+      R divU = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+      for (int i = 0; i < 3; ++i) {
+        R r = R(0.5) * (divF[i] + ul[gp * 3 + i] * divU);
+        for (int j = 0; j < 3; ++j) r = r + R(0.5) * (ul[gp * 3 + j] * gradQ[i][j]);
+        buf[((size_t)e * n + gp) * 3 + i] = GV(g, m, gp, e) * r;
+      }
+    }
+  }
+  R *dst[3] = {Rmom, Rmom + N, Rmom + 2 * N};
+  scatter(m, buf, 3, dst, R(1));
+}
+
+// ---- conjGrad_pressure_incomp, src/lib_sod2d_incomp/sources/mod_solver_incomp.f90:253-506
+// Jacobi-preconditioned CG on A x = R - A x0 with FP64 dot products and the
+// Polak-Ribiere beta of the reference; vectors in R (FP32 in the reference),
+// alpha and beta rounded to R.  Owned nodes = working nodes on one rank.
+// Returns the iteration count; *res_rel = ||r|| / ||b|| at exit.
+template <class R>
+int conjGrad_pressure(const Mesh &m, const Geo<R> &g, const R *diag, const R *x0, const R *Rhs, int maxIter,
+                      double tol, R *out, double *res_rel) {
+  const long long N = m.npoin;
+  std::vector<R> x(N, 0), r0(N, 0), p0(N, 0), qn(N, 0), b(N, 0), z0(N, 0), z1(N, 0);
+  eval_laplacian_mult(m, g, x0, qn.data());
+  for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; b[p] = Rhs[p] - qn[p]; }
+  for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; r0[p] = b[p]; }
+  for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; z0[p] = r0[p] / diag[p]; p0[p] = z0[p]; }
+  double auxT1 = 0.0;
+  for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; auxT1 += (double)(b[p] * b[p]); }
+  const double auxB = std::sqrt(auxT1);
+  int iter;
+  double nrm = auxB;
+  for (iter = 1; iter <= maxIter; ++iter) {
+    eval_laplacian_mult(m, g, p0.data(), qn.data());
+    double Q1 = 0.0, Q2 = 0.0;
+    for (int t = 0; t < m.npoin_w; ++t) {
+      int p = m.lpoin_w[t] - 1;
+      Q1 += (double)(r0[p] * z0[p]);
+      Q2 += (double)(p0[p] * qn[p]);
+    }
+    R alpha = (R)(Q1 / Q2);
+    for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; x[p] = x[p] + alpha * p0[p]; }
+    for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; r0[p] = r0[p] - alpha * qn[p]; }
+    for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; z1[p] = z0[p]; z0[p] = r0[p] / diag[p]; }
+    auxT1 = 0.0;
+    for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; auxT1 += (double)(r0[p] * r0[p]); }
+    nrm = std::sqrt(auxT1);
+    if (nrm < tol * auxB) break;
+    double T = 0.0;
+    for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; T += (double)(r0[p] * (z0[p] - z1[p])); }
+    R beta = (R)(T / Q1);
+    for (int t = 0; t < m.npoin_w; ++t) { int p = m.lpoin_w[t] - 1; p0[p] = z0[p] + beta * p0[p]; }
+  }
+  for (long long p = 0; p < N; ++p) out[p] = x0[p] + x[p];
+  *res_rel = auxB > 0 ? nrm / auxB : 0.0;
+  return iter > maxIter ? maxIter : iter;
+}
+
 }  // namespace oracle

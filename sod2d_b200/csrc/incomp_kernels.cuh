@@ -1,0 +1,254 @@
+// Kernels of the incompressible pressure path: matrix-free Laplacian
+// (eval_laplacian_mult), its Jacobi diagonal, gradient, divergence,
+// skew-symmetric convection, and the vector kernels of the (flexible)
+// conjugate-gradient solvers with deterministic FP64 reductions.
+#pragma once
+#include "rhs_kernels.cuh"
+
+namespace sod {
+
+// ---- Laplacian: ResP = sum_e int grad N . grad p  (mod_operators.f90:16-112)
+// One thread per Gauss point; V = float (reference arithmetic) or double.
+// Writes one V per element node into slots (width 1).
+template <int P, int EPB, class V>
+__global__ void __launch_bounds__(EPB *Cfg<P>::NT)
+k_lap_elem(MeshDev m, const V *__restrict__ p, V *__restrict__ slots) {
+  constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
+  __shared__ V sm[EPB][4][N];
+  const int el = threadIdx.x / NT, t = threadIdx.x % NT;
+  const long long e = (long long)blockIdx.x * EPB + el;
+  const bool active = (e < m.nelem) && (t < N);
+  if (active) sm[el][0][t] = p[m.conn[e * N + t]];
+  __syncthreads();
+  const int i = t % N1, j = (t / N1) % N1, k = t / (N1 * N1);
+  V C0 = 0, C1 = 0, C2 = 0;
+  V Di[N1], Dj[N1], Dk[N1];
+  if (active) {
+#pragma unroll
+    for (int s = 0; s < N1; ++s) {
+      Di[s] = (V)m.Dnat[i * N1 + s]; Dj[s] = (V)m.Dnat[j * N1 + s]; Dk[s] = (V)m.Dnat[k * N1 + s];
+    }
+    const float *g = m.geo + e * 10 * N + t;
+    V He[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) He[c] = (V)g[c * N];
+    const V gv = (V)g[9 * N];
+    const V *f = sm[el][0];
+    V g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int s = 0; s < N1; ++s) {
+      const int mm = ref_order<P>(s);
+      g0 += Di[mm] * f[mm + N1 * j + N1 * N1 * k];
+      g1 += Dj[mm] * f[i + N1 * mm + N1 * N1 * k];
+      g2 += Dk[mm] * f[i + N1 * j + N1 * N1 * mm];
+    }
+    V gP[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) gP[a] = He[a] * g0 + He[a + 3] * g1 + He[a + 6] * g2;
+    C0 = gv * (He[0] * gP[0] + He[1] * gP[1] + He[2] * gP[2]);
+    C1 = gv * (He[3] * gP[0] + He[4] * gP[1] + He[5] * gP[2]);
+    C2 = gv * (He[6] * gP[0] + He[7] * gP[1] + He[8] * gP[2]);
+  }
+  __syncthreads();
+  if (active) { sm[el][1][t] = C0; sm[el][2][t] = C1; sm[el][3][t] = C2; }
+  __syncthreads();
+  if (!active) return;
+  V acc = 0;
+#pragma unroll
+  for (int s = 0; s < N1; ++s) {
+    const int mm = ref_order<P>(s);
+    acc += (V)m.Dnat[mm * N1 + i] * sm[el][1][mm + N1 * j + N1 * N1 * k];
+    acc += (V)m.Dnat[mm * N1 + j] * sm[el][2][i + N1 * mm + N1 * N1 * k];
+    acc += (V)m.Dnat[mm * N1 + k] * sm[el][3][i + N1 * j + N1 * N1 * mm];
+  }
+  slots[e * N + t] = acc;
+}
+
+// Scalar-slot assembly out(p) = scale * sum(slots of p); float sums are
+// Kahan-compensated.  Only nodes with slots are written (masters).
+template <class V>
+__global__ void k_gather1(MeshDev m, const V *__restrict__ slots, V *__restrict__ out, int use_invMl) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= m.npoin) return;
+  const int b = m.slot_ptr[p], en = m.slot_ptr[p + 1];
+  V sum = 0, cmp = 0;
+  for (int s = b; s < en; ++s) {
+    const V y = slots[m.slot_idx[s]] - cmp;
+    const V tt = sum + y;
+    cmp = (tt - sum) - y;
+    sum = tt;
+  }
+  out[p] = use_invMl ? sum * (V)m.invMl[p] : sum;
+}
+
+// ---- eval_laplacian_diag, mod_operators.f90:638-682 --------------------
+// d(a) = sum_g gpvol(g) |grad N_a(g)|^2; with GLL collocation grad N_a(g)
+// is non-zero only on the three lines through a.  One thread per node a
+// of an element loops over the Gauss points of those lines.
+template <int P>
+__global__ void k_lap_diag_elem(MeshDev m, float *__restrict__ slots) {
+  constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)m.nelem * N) return;
+  const long long e = idx / N;
+  const int a = (int)(idx % N);
+  const int ia = a % N1, ja = (a / N1) % N1, ka = a / (N1 * N1);
+  const float *g = m.geo + e * 10 * N;
+  float d = 0.f;
+  for (int gp = 0; gp < N; ++gp) {
+    const int i = gp % N1, j = (gp / N1) % N1, k = gp / (N1 * N1);
+    // iso-derivatives of N_a at gp: D[i][ia] d_{j,ja} d_{k,ka}, ...
+    float d0 = (j == ja && k == ka) ? m.Dnat[i * N1 + ia] : 0.f;
+    float d1 = (i == ia && k == ka) ? m.Dnat[j * N1 + ja] : 0.f;
+    float d2 = (i == ia && j == ja) ? m.Dnat[k * N1 + ka] : 0.f;
+    if (d0 == 0.f && d1 == 0.f && d2 == 0.f) continue;
+    const float gv = g[9 * N + gp];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float gc = g[c * N + gp] * d0 + g[(c + 3) * N + gp] * d1 + g[(c + 6) * N + gp] * d2;
+      d += gv * gc * gc;
+    }
+  }
+  slots[idx] = d;
+}
+
+// ---- gradient / divergence / incompressible convection ----------------
+// MODE 0: gradient of a scalar x: slots (width 4) = gpvol*grad x (3)
+// MODE 1: divergence of u: slot[0] = gpvol * div u
+// MODE 2: full_convec_ijk_incomp (elem_convec_incomp.f90:19-125): slots
+//         (width 4) = gpvol * 0.5*(div(q u) + u div q + (u.grad) q)
+template <int P, int EPB, int MODE>
+__global__ void __launch_bounds__(EPB *Cfg<P>::NT)
+k_vec_elem(MeshDev m, const float *__restrict__ x, const float *__restrict__ u, const float *__restrict__ q,
+           float *__restrict__ slots) {
+  constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
+  constexpr int NF = MODE == 0 ? 1 : (MODE == 1 ? 3 : 12);
+  __shared__ float sm[EPB][NF][N];
+  const int el = threadIdx.x / NT, t = threadIdx.x % NT;
+  const long long e = (long long)blockIdx.x * EPB + el;
+  const bool active = (e < m.nelem) && (t < N);
+  const long long NP = m.npoin;
+  float ul[3] = {0.f, 0.f, 0.f}, ql[3] = {0.f, 0.f, 0.f};
+  if (active) {
+    const int node = m.conn[e * N + t];
+    if (MODE == 0) sm[el][0][t] = x[node];
+    if (MODE >= 1)
+      for (int d = 0; d < 3; ++d) { ul[d] = u[node + NP * d]; sm[el][d][t] = (MODE == 1) ? ul[d] : 0.f; }
+    if (MODE == 2) {
+      for (int d = 0; d < 3; ++d) { ql[d] = q[node + NP * d]; sm[el][d][t] = ql[d]; }
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) sm[el][3 + a * 3 + b][t] = ql[a] * ul[b];
+    }
+  }
+  __syncthreads();
+  if (!active) return;
+  const int i = t % N1, j = (t / N1) % N1, k = t / (N1 * N1);
+  float Di[N1], Dj[N1], Dk[N1];
+#pragma unroll
+  for (int s = 0; s < N1; ++s) { Di[s] = m.Dnat[i * N1 + s]; Dj[s] = m.Dnat[j * N1 + s]; Dk[s] = m.Dnat[k * N1 + s]; }
+  const float *g = m.geo + e * 10 * N + t;
+  float He[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) He[c] = g[c * N];
+  const float gv = g[9 * N];
+  float out[3] = {0.f, 0.f, 0.f};
+  float a0, a1, a2;
+  if (MODE == 0) {
+    iso_grad<P>(sm[el][0], i, j, k, Di, Dj, Dk, a0, a1, a2);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[a] = gv * (He[a] * a0 + He[a + 3] * a1 + He[a + 6] * a2);
+  } else if (MODE == 1) {
+    float dv = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      iso_grad<P>(sm[el][c], i, j, k, Di, Dj, Dk, a0, a1, a2);
+      dv += He[c] * a0 + He[c + 3] * a1 + He[c + 6] * a2;
+    }
+    out[0] = gv * dv;
+  } else {
+    float gradQ[3][3], divF[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      iso_grad<P>(sm[el][c], i, j, k, Di, Dj, Dk, a0, a1, a2);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) gradQ[c][b] = He[b] * a0 + He[b + 3] * a1 + He[b + 6] * a2;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        iso_grad<P>(sm[el][3 + a * 3 + b], i, j, k, Di, Dj, Dk, a0, a1, a2);
+        divF[a] += He[b] * a0 + He[b + 3] * a1 + He[b + 6] * a2;
+      }
+    const float divU = gradQ[0][0] + gradQ[1][1] + gradQ[2][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float r = 0.5f * (divF[a] + ul[a] * divU);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) r = r + 0.5f * (ul[b] * gradQ[a][b]);
+      out[a] = gv * r;
+    }
+  }
+  reinterpret_cast<float4 *>(slots + (e * N + t) * 4)[0] = make_float4(out[0], out[1], out[2], 0.f);
+}
+
+// ---- CG vector kernels (FP64 reductions, deterministic) ---------------
+// Block partial sums of up to 3 dot products over working nodes; a second
+// single-block kernel sums the partials in a fixed order.
+constexpr int DOT_BLOCKS = 592;  // 4 blocks per SM on 148 SMs
+constexpr int DOT_THREADS = 256;
+
+// dot d = sum a[d]*(b[d] - c[d]) (c[d] may be null)
+template <class V, int ND>
+struct DotArgs {
+  const V *a[ND];
+  const V *b[ND];
+  const V *c[ND];
+};
+
+template <class V, int ND>
+__global__ void k_dot_partial(int npoin_w, const int *__restrict__ lpoin_w, DotArgs<V, ND> A,
+                              double *__restrict__ part) {
+  __shared__ double sh[ND][DOT_THREADS];
+  double s[ND];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) s[d] = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npoin_w; t += gridDim.x * blockDim.x) {
+    const int p = lpoin_w[t];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const V bb = A.c[d] ? (V)(A.b[d][p] - A.c[d][p]) : A.b[d][p];
+      s[d] += (double)(A.a[d][p] * bb);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < ND; ++d) sh[d][threadIdx.x] = s[d];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int d = 0; d < ND; ++d) part[d * DOT_BLOCKS + blockIdx.x] = sh[d][0];
+}
+
+__global__ void k_dot_final(int nd, const double *__restrict__ part, double *__restrict__ out) {
+  __shared__ double sh[1024];
+  for (int d = 0; d < nd; ++d) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < DOT_BLOCKS; b += blockDim.x) s += part[d * DOT_BLOCKS + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[d] = sh[0];
+    __syncthreads();
+  }
+}
+
+}  // namespace sod

@@ -143,3 +143,60 @@ class Context:
     @property
     def device_bytes(self) -> int:
         return int(lib().sod_gpu_device_bytes(self.h))
+
+
+class CompSolver:
+    """Compressible periodic time loop on the GPU through the C-ABI: the
+    driver logic of CFDSolverBase_evalTimeIteration
+    (src/lib_mainBaseClass/sources/CFDSolverBase.f90:1929-2164) around
+    sod_gpu_comp_rk_ls_step."""
+
+    def __init__(self, mesh, ic, stages=4, rk_n=1, fp64_state=True, cfl_conv=0.5, cfl_diff=0.5):
+        import torch
+        self.torch = torch
+        self.ctx = Context(mesh, phys_from_ic(ic))
+        self.mesh, self.ic = mesh, ic
+        self.cfl = (cfl_conv, cfl_diff)
+        dv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        self._init = [dv(a) for a in (ic.rho, ic.u, ic.q, ic.pr, ic.E, ic.Tem, ic.csound, ic.machno, ic.eta)]
+        cfg = RkCfg(stages, rk_n, int(fp64_state), ic.mu_factor)
+        self.ctx.call("sod_gpu_comp_init_state", C.byref(cfg), *(dptr(t) for t in self._init))
+        self.time = np.float32(0.0)
+        self.dt = self.adapt_dt()
+
+    def adapt_dt(self) -> float:
+        v = C.c_float()
+        self.ctx.call("sod_gpu_comp_adapt_dt", self.cfl[0], self.cfl[1], C.byref(v))
+        return float(v.value)
+
+    def analysis(self):
+        out = (C.c_double * 5)()
+        self.ctx.call("sod_gpu_comp_analysis", float(self.ic.rho0), out)
+        return [float(self.time)] + list(out)
+
+    def step(self):
+        self.ctx.call("sod_gpu_comp_rk_ls_step", float(self.dt))
+        self.time = np.float32(self.time + np.float32(self.dt))
+
+    def run(self, nsteps, log_first=1, log_step=10, max_time=None):
+        hist = [self.analysis()]
+        log_next = log_first
+        for istep in range(1, nsteps + 1):
+            self.step()
+            if istep == log_next:
+                hist.append(self.analysis())
+                log_next += log_step
+            self.dt = self.adapt_dt()
+            if max_time is not None and self.time >= np.float32(max_time):
+                break
+        return np.array(hist)
+
+    def state(self):
+        torch = self.torch
+        N, n, E = self.mesh.npoin, self.mesh.nnode, self.mesh.nelem
+        t = [torch.zeros(k, device="cuda") for k in (N, 3 * N, N, E * n)]
+        self.ctx.call("sod_gpu_comp_get_state", *(dptr(x) for x in t))
+        return dict(zip(("rho", "q", "E", "mu_e"), (x.cpu().numpy() for x in t)))
+
+    def close(self):
+        self.ctx.close()
