@@ -27,6 +27,14 @@ class SodMesh(C.Structure):
                 ("helem", VP), ("helem_l", VP), ("lelpn", VP), ("Ngp", VP)]
 
 
+class SolveOpts(C.Structure):
+    _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("precond", C.c_int), ("stagnation_window", C.c_int)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("fallback", C.c_int), ("res_rel", C.c_double), ("seconds", C.c_double)]
+
+
 class RkCfg(C.Structure):
     _fields_ = [("stages", C.c_int), ("rk_n", C.c_int), ("fp64_state", C.c_int), ("mu_factor", C.c_float)]
 
@@ -58,6 +66,15 @@ SIGNATURES = {
     "sod_gpu_comp_adapt_dt": (C.c_int, [VP, C.c_float, C.c_float, C.POINTER(C.c_float)]),
     "sod_gpu_comp_analysis": (C.c_int, [VP, C.c_float, C.POINTER(C.c_double)]),
     "sod_gpu_comp_get_state": (C.c_int, [VP] + [VP] * 4),
+    "sod_gpu_eval_laplacian_mult": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_eval_laplacian_mult64": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_eval_laplacian_diag": (C.c_int, [VP, VP]),
+    "sod_gpu_eval_gradient": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_eval_divergence": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_full_convec_ijk_incomp": (C.c_int, [VP, VP, VP, VP]),
+    "sod_gpu_conjgrad_pressure": (C.c_int, [VP, VP, VP, C.c_int, C.c_double, C.POINTER(C.c_int),
+                                            C.POINTER(C.c_double)]),
+    "sod_gpu_pressure_solve": (C.c_int, [VP, VP, VP, VP, VP]),
 }
 
 
