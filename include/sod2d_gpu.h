@@ -226,6 +226,32 @@ int sod_gpu_comp_analysis(sod_gpu_ctx *ctx, float rho0, double *out);
  * be NULL): rho, q(N,3), E and mu_e(nelem,ngaus). */
 int sod_gpu_comp_get_state(sod_gpu_ctx *ctx, float *rho, float *q, float *E, float *mu_e);
 
+/* ---- allocation-free analysis integrals ---------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a solver whose device memory belongs to its own pool or is
+ * capped, code running during CUDA-graph stream capture, callers that must
+ * not let cudaMalloc synchronise the device inside the time loop), this
+ * computes the same integrals as sod_gpu_comp_analysis without a context:
+ * every input is a device pointer in the reference layout (connec, lpoin_w
+ * 1-based; He(3,3,ngaus,nelem), gpvol, dlxigp_ip, Ngp (may be NULL), rho,
+ * u(npoin,3), mu_fluid, mu_e(nelem,ngaus), machno) and out[0..4] (host)
+ * receives EK, eps_S, eps_D, eps_T, max Mach.  volT is the domain volume.
+ * It allocates nothing: its scratch is a fixed __device__ array of
+ * SOD_NOALLOC_MAX_ELEM x 3 floats (12 MiB) that each GPU loading the
+ * library keeps until the process exits; larger meshes are rejected with
+ * SOD_GPU_EINVAL.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU
+ * race; serialise them.  Work is enqueued on `stream` (NULL = default) and
+ * the call returns after the results have been copied to out. */
+#define SOD_NOALLOC_MAX_ELEM (1 << 20)
+int sod_gpu_analysis_noalloc(int porder, int nelem, int npoin, int npoin_w, const int *connec,
+                             const int *lpoin_w, const int *invAtoIJK, const int *gmshAtoI,
+                             const int *gmshAtoJ, const int *gmshAtoK, const float *dlxigp_ip,
+                             const float *He, const float *gpvol, const float *Ngp, const float *rho,
+                             const float *u, const float *mu_fluid, const float *mu_e,
+                             const float *machno, float rho0, float volT, void *stream, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,7 @@ NVCC = os.environ.get("SOD2D_NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 HOST_SRCS = ["host_setup.cpp"]
-GPU_SRCS = ["sod2d_gpu.cu"]
+GPU_SRCS = ["sod2d_gpu.cu", "noalloc_analysis.cu"]
 
 
 def _stale(target: Path, deps) -> bool:

@@ -34,6 +34,10 @@ inline int nat_of(int porder, int ii) { return ii == 0 ? 0 : (ii == 1 ? porder :
 
 }  // namespace
 
+// Records an error message for sod_gpu_last_error() from other translation
+// units of the library.
+int sod_detail_set_error(int code, const char *msg) { return fail(code, msg); }
+
 struct sod_gpu_ctx {
   int P = 0, N1 = 0, N = 0, nelem = 0, npoin = 0, npoin_w = 0;
   cudaStream_t stream = 0;

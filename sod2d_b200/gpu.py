@@ -75,6 +75,8 @@ SIGNATURES = {
     "sod_gpu_conjgrad_pressure": (C.c_int, [VP, VP, VP, C.c_int, C.c_double, C.POINTER(C.c_int),
                                             C.POINTER(C.c_double)]),
     "sod_gpu_pressure_solve": (C.c_int, [VP, VP, VP, VP, VP]),
+    "sod_gpu_analysis_noalloc": (C.c_int, [C.c_int] * 4 + [VP] * 15 + [C.c_float, C.c_float, VP,
+                                                                       C.POINTER(C.c_double)]),
 }
 
 
