@@ -183,6 +183,8 @@ typedef struct {
   double tol;
   int precond;         /* 0 Jacobi, 1 learned                                */
   int stagnation_window; /* iterations without a 2x residual drop -> fallback */
+  int harvest;         /* 1: record (residual, error) pairs of this solve for
+                          training the learned preconditioner             */
 } sod_solve_opts_t;
 typedef struct {
   int iterations;
@@ -192,6 +194,48 @@ typedef struct {
 } sod_solve_stats_t;
 int sod_gpu_pressure_solve(sod_gpu_ctx *ctx, const double *b, double *x, const sod_solve_opts_t *opts,
                            sod_solve_stats_t *stats);
+
+/* ---- learned element-patch preconditioner (no counterpart in the reference)
+ * Per element: the Jacobi-scaled residual on its nodes and the element means
+ * of its 6 face neighbours, scaled to unit RMS, pass through a 32-32 tanh
+ * MLP whose output corrects the Jacobi step on the element's nodes; element
+ * outputs are averaged at shared nodes.  With a zero output layer (the
+ * initial state) it is exactly Jacobi.  Trained on the GPU by this library's
+ * own forward, backward and Adam kernels to minimise the energy norm
+ * ||e - M(r)||_A^2 / ||e||_A^2 over (residual, error) pairs harvested from
+ * the library's Jacobi pressure solves. */
+int sod_gpu_precond_num_params(sod_gpu_ctx *ctx);
+/* Allocates the network and a harvest ring of `harvest_capacity` pairs and
+ * sets seeded initial parameters. */
+int sod_gpu_precond_init(sod_gpu_ctx *ctx, uint64_t seed, int harvest_capacity);
+int sod_gpu_precond_set_params(sod_gpu_ctx *ctx, const float *host_params, int n);
+int sod_gpu_precond_get_params(sod_gpu_ctx *ctx, float *host_params, int n);
+/* z = M(r) on working nodes (device FP64 vectors). */
+int sod_gpu_precond_apply(sod_gpu_ctx *ctx, const double *r, double *z);
+/* Loss ||e - M(r)||_A^2/||e||_A^2 (host *loss) and its parameter gradient
+ * (host grad, nparam floats, may be NULL) for one pair; no update. */
+int sod_gpu_precond_loss_grad(sod_gpu_ctx *ctx, const double *r, const double *e, double *loss,
+                              float *grad_host);
+/* Number of harvested pairs available for training. */
+int sod_gpu_precond_harvest_count(sod_gpu_ctx *ctx);
+/* Adam: `steps` updates over mini-batches of `batch` (<= 16) harvested
+ * pairs; *final_loss (host) = mean loss of the last batch. */
+int sod_gpu_precond_train(sod_gpu_ctx *ctx, int steps, int batch, float lr, uint64_t seed, float *final_loss);
+
+/* ---- incompressible projection step (pressure-system generator) --------
+ * A first-order explicit projection step of the periodic incompressible
+ * Navier-Stokes equations built from the operators above:
+ *   u* = u - dt (C(u) + nu L u) / Ml   (C: full_convec_ijk_incomp, L: Laplacian)
+ *   A p = -div(u*)/dt,  p0 = 2 p^n - p^(n-1) (extrapolated from the previous
+ *   two pressures), solved by sod_gpu_pressure_solve
+ *   u = u* - dt grad p
+ * It stands in for the reference's BDF/EXT3 step with its implicit velocity
+ * solve (time_integ_incomp.f90:88-434) as a source of the time sequence of
+ * pressure-Poisson systems. */
+int sod_gpu_incomp_init(sod_gpu_ctx *ctx, const float *u, double nu);
+int sod_gpu_incomp_step(sod_gpu_ctx *ctx, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats);
+/* Copies of the current velocity u(npoin,3) (FP32) and pressure (FP64); NULL skips. */
+int sod_gpu_incomp_get(sod_gpu_ctx *ctx, float *u, double *p);
 
 /* ---- compressible time integration with library-owned state ----------
  * The conserved state lives on the device in FP64 (fp64_state = 1) or in

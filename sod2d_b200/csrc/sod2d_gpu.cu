@@ -4,6 +4,7 @@
 #include "rhs_kernels.cuh"
 #include "step_kernels.cuh"
 #include "incomp_kernels.cuh"
+#include "precond_net.cuh"
 
 #include <cuda_runtime.h>
 
@@ -11,6 +12,11 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <map>
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <random>
 
 using namespace sod;
 
@@ -65,6 +71,30 @@ struct sod_gpu_ctx {
     double *x, *r, *p, *q, *z0, *z1, *b, *Minv;                // FP64 CG
     double *part, *dots;                                        // reductions
   } cg;
+  // learned preconditioner
+  struct Net {
+    bool ready = false;
+    int nparam = 0, nblk_bwd = 0, bwd_threads = 256, step = 0;
+    float *params = nullptr, *m1 = nullptr, *m2 = nullptr, *part = nullptr, *wts = nullptr, *emean = nullptr,
+          *act = nullptr, *grad = nullptr;
+    int *nbr = nullptr;
+    // harvest ring of (r, e) pairs, FP32, and e^T A e per pair
+    int cap = 0, count = 0, next = 0;
+    float *hr = nullptr, *he = nullptr;
+    std::vector<double> eAe;
+    double *xsnap = nullptr;  // solver snapshots (FP64) while harvesting
+    double *tmp1 = nullptr, *tmp2 = nullptr;
+    float *zf = nullptr;
+    int harvest_every_solve = 0;
+  } net;
+  // incompressible projection-step state
+  struct Inc {
+    bool ready = false;
+    float *u = nullptr, *ustar = nullptr, *R = nullptr, *L = nullptr, *div = nullptr, *grad = nullptr, *pf = nullptr;
+    double *p = nullptr, *pold = nullptr, *b = nullptr, *x = nullptr;
+    double nu = 0.0;
+    int nsteps = 0;
+  } inc;
   // compressible time-integration state
   struct Comp {
     bool ready = false, fp64 = true, first = true;
@@ -733,6 +763,9 @@ namespace {
 
 int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z);  // defined with the network
 
+__global__ void k_d2f_w(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ a,
+                        float *__restrict__ b);
+
 __global__ void k_sub_mean(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ sum_in,
                            double *__restrict__ b) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -753,6 +786,14 @@ __global__ void k_ones_dot(int npoin_w, const int *__restrict__ lpoin_w, const d
     __syncthreads();
   }
   if (threadIdx.x == 0) part[0] = sh[0];
+}
+
+__global__ void k_copy_cast_w(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ a,
+                              double *__restrict__ b) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  b[i] = (double)a[i];
 }
 
 __global__ void k_jacobi64(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ Minv,
@@ -804,6 +845,21 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
   int it = 0, fallback = 0;
   double res = 0.0;
   const int window = opts->stagnation_window > 0 ? opts->stagnation_window : 50;
+  auto &NT = c->net;
+  const bool harvest = opts->harvest && NT.ready && NT.cap > 0 && kind == 0;
+  std::vector<std::pair<int, int>> snaps;  // (ring slot, snapshot index)
+  int next_snap = 0;
+  auto take_snapshot = [&](int iter_no) {
+    if (!harvest || (int)snaps.size() >= 16 || iter_no != next_snap) return;
+    next_snap = next_snap == 0 ? 1 : next_snap * 2;
+    const int slot = NT.next;
+    NT.next = (NT.next + 1) % NT.cap;
+    if (NT.count < NT.cap) NT.count++;
+    const int si = (int)snaps.size();
+    k_d2f_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.r, NT.hr + (size_t)slot * N);
+    cudaMemcpyAsync(NT.xsnap + (size_t)si * N, x, N * 8, cudaMemcpyDeviceToDevice, st);
+    snaps.push_back({slot, si});
+  };
   if (bnorm == 0.0) {
     CUDA_TRY(cudaMemsetAsync(x, 0, N * 8, st));
   } else {
@@ -816,6 +872,7 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
       k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, G.z0, 0.0, G.p);
       double best = 1e300;
       int best_it = it;
+      take_snapshot(it);
       for (; it < opts->max_iter;) {
         ++it;
         lap<double>(c, G.p, G.q);
@@ -849,8 +906,22 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
         }
         k_cg_update2<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.dots, G.dots + 2, G.p, G.z0);
         res = nrm;
+        take_snapshot(it);
       }
     }
+  }
+  // harvested pairs: e_k = x* - x_k and their energy norms
+  for (auto &sn : snaps) {
+    double *e = NT.tmp1;
+    k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, x, 0.0, e);
+    k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, -1.0, NT.xsnap + (size_t)sn.second * N, 1.0, e);
+    k_d2f_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, e, NT.he + (size_t)sn.first * N);
+    lap<double>(c, e, NT.tmp2);
+    dots<double, 1>(c, DotArgs<double, 1>{{e}, {NT.tmp2}, {nullptr}}, G.dots + 5);
+    double eAe = 0.0;
+    CUDA_TRY(cudaMemcpyAsync(&eAe, G.dots + 5, 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    NT.eAe[sn.first] = eAe > 0 ? eAe : 1.0;
   }
   CUDA_TRY(cudaEventRecord(e1, st));
   CUDA_TRY(cudaEventSynchronize(e1));
@@ -877,7 +948,21 @@ int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z) {
     k_jacobi64<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, c->cg.Minv, r, z);
     return 0;
   }
-  return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
+  auto &NT = c->net;
+  if (!NT.ready) return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
+  k_elem_mean<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), c->N, r, c->cg.Minv, NT.emean);
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    constexpr int P = LL::P_;
+    using D = NetDims<P>;
+    const size_t sm = (size_t)(D::NPARAM + 8 * (D::NIN + 2 * NET_H)) * 4;
+    k_net_fwd<P, false><<<592, 256, sm, c->stream>>>(c->md(), NT.nbr, NT.emean, r, c->cg.Minv, NT.wts, NT.params,
+                                                     c->slotsB, nullptr);
+    return 0;
+  });
+  k_gather1<float><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, NT.zf, 0);
+  k_copy_cast_w<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, NT.zf, z);
+  return 0;
 }
 
 }  // namespace
@@ -1179,6 +1264,390 @@ int sod_gpu_comp_get_state(sod_gpu_ctx *c, float *rho, float *q, float *E, float
     const long long EN = (long long)c->nelem * c->N;
     k_t_to_elem<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, c->mue_t, mu_e);
   }
+  return c->finish();
+}
+
+}  // extern "C"
+
+// ---- learned preconditioner: set-up, loss/gradient, harvest, training ----
+
+namespace {
+
+template <int P>
+size_t bwd_smem(int nwarps) {
+  using D = NetDims<P>;
+  return (size_t)(D::NPARAM + D::N * NET_H + NET_H * NET_H + nwarps * D::NPARAM + nwarps * (D::N + 2 * NET_H)) * 4;
+}
+
+// Forward (training), z = assembled output at working nodes (FP64).
+void net_forward_train(sod_gpu_ctx *c, const double *r, double *z) {
+  auto &NT = c->net;
+  k_elem_mean<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), c->N, r, c->cg.Minv, NT.emean);
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    constexpr int P = LL::P_;
+    using D = NetDims<P>;
+    const size_t sm = (size_t)(D::NPARAM + 8 * (D::NIN + 2 * NET_H)) * 4;
+    k_net_fwd<P, true><<<592, 256, sm, c->stream>>>(c->md(), NT.nbr, NT.emean, r, c->cg.Minv, NT.wts, NT.params,
+                                                    c->slotsB, NT.act);
+    return 0;
+  });
+  k_gather1<float><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, NT.zf, 0);
+  k_copy_cast_w<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, NT.zf, z);
+}
+
+void net_backward(sod_gpu_ctx *c, const double *g, float *part) {
+  auto &NT = c->net;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    constexpr int P = LL::P_;
+    const int nw = NT.bwd_threads / 32;
+    k_net_bwd<P><<<NT.nblk_bwd, NT.bwd_threads, bwd_smem<P>(nw), c->stream>>>(c->md(), g, NT.wts, NT.params,
+                                                                             NT.act, part);
+    return 0;
+  });
+}
+
+__global__ void k_loss_grad_vec(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ Ad,
+                                double scale, double *__restrict__ g) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  g[i] = scale * Ad[i];
+}
+
+__global__ void k_f2d_w(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ a,
+                        double *__restrict__ b) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  b[i] = (double)a[i];
+}
+
+__global__ void k_d2f_w(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ a,
+                        float *__restrict__ b) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  b[i] = (float)a[i];
+}
+
+// loss = d^T A d / eAe with d = e - z; writes g = dL/dz = -2 A d / eAe into
+// NT.tmp2, and the per-block parameter-gradient partials into part.
+int net_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double eAe, float *part, double *loss) {
+  auto &NT = c->net;
+  auto &G = c->cg;
+  const int nw = c->npoin_w;
+  const unsigned nb = nblk(nw, 256);
+  net_forward_train(c, r, NT.tmp1);                                            // z
+  k_axpby<double><<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, 1.0, e, -1.0, NT.tmp1);  // d = e - z
+  lap<double>(c, NT.tmp1, NT.tmp2);                                            // A d
+  dots<double, 1>(c, DotArgs<double, 1>{{NT.tmp1}, {NT.tmp2}, {nullptr}}, G.dots + 2);
+  k_loss_grad_vec<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, NT.tmp2, -2.0 / eAe, NT.tmp2);
+  net_backward(c, NT.tmp2, part);
+  if (loss) {
+    double h;
+    CUDA_TRY(cudaMemcpyAsync(&h, G.dots + 2, 8, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *loss = h / eAe;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sod_gpu_precond_num_params(sod_gpu_ctx *c) {
+  if (!c) return fail(SOD_GPU_EINVAL, "null context");
+  return c->P == 3 ? NetDims<3>::NPARAM : NetDims<4>::NPARAM;
+}
+
+int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
+  if (!c || harvest_capacity < 0) return fail(SOD_GPU_EINVAL, "bad argument");
+  int rc;
+  if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c))) return rc;
+  auto &NT = c->net;
+  const int N = c->N, P = c->P;
+  const long long E = c->nelem;
+  if (!NT.ready) {
+    NT.nparam = sod_gpu_precond_num_params(c);
+    NT.bwd_threads = P == 3 ? 256 : 128;
+    NT.nblk_bwd = 148;
+    const int nact = P == 3 ? NetDims<3>::NACT : NetDims<4>::NACT;
+    if ((rc = c->alloc(&NT.params, NT.nparam)) || (rc = c->alloc(&NT.m1, NT.nparam)) ||
+        (rc = c->alloc(&NT.m2, NT.nparam)) || (rc = c->alloc(&NT.grad, NT.nparam)) ||
+        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.wts, (size_t)E * N)) ||
+        (rc = c->alloc(&NT.emean, (size_t)E)) || (rc = c->alloc(&NT.act, (size_t)E * nact)) ||
+        (rc = c->alloc(&NT.nbr, (size_t)E * 6)) || (rc = c->alloc(&NT.tmp1, (size_t)c->npoin)) ||
+        (rc = c->alloc(&NT.tmp2, (size_t)c->npoin)) || (rc = c->alloc(&NT.zf, (size_t)c->npoin)))
+      return rc;
+    const size_t smb = P == 3 ? bwd_smem<3>(8) : bwd_smem<4>(4);
+    if (P == 3) {
+      CUDA_TRY(cudaFuncSetAttribute(k_net_bwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+    } else {
+      CUDA_TRY(cudaFuncSetAttribute(k_net_bwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+    }
+    // connectivity back on the host: face neighbours and assembly weights
+    std::vector<int> conn((size_t)E * N), lel(c->npoin, 0);
+    CUDA_TRY(cudaMemcpy(conn.data(), c->conn, conn.size() * 4, cudaMemcpyDeviceToHost));
+    for (long long e = 0; e < E; ++e)
+      for (int t = 0; t < N; ++t) lel[conn[e * N + t]]++;
+    std::vector<float> w((size_t)E * N);
+    for (long long e = 0; e < E; ++e)
+      for (int t = 0; t < N; ++t) w[e * N + t] = 1.0f / (float)lel[conn[e * N + t]];
+    const int N1 = c->N1, Pm = P;
+    auto tid = [&](int i, int j, int k) { return i + N1 * (j + N1 * k); };
+    std::map<std::array<int, 4>, std::vector<std::pair<long long, int>>> faces;
+    for (long long e = 0; e < E; ++e)
+      for (int f = 0; f < 6; ++f) {
+        const int d = f / 2, v = (f % 2) ? Pm : 0;
+        std::array<int, 4> key;
+        int q = 0;
+        for (int a = 0; a <= Pm; a += Pm)
+          for (int b = 0; b <= Pm; b += Pm) {
+            int i = 0, j = 0, k = 0;
+            if (d == 0) { i = v; j = a; k = b; }
+            if (d == 1) { i = a; j = v; k = b; }
+            if (d == 2) { i = a; j = b; k = v; }
+            key[q++] = conn[e * N + tid(i, j, k)];
+          }
+        std::sort(key.begin(), key.end());
+        faces[key].push_back({e, f});
+      }
+    std::vector<int> nbr((size_t)E * 6);
+    for (long long e = 0; e < E; ++e)
+      for (int f = 0; f < 6; ++f) nbr[e * 6 + f] = (int)e;
+    for (auto &kv : faces) {
+      auto &v = kv.second;
+      if (v.size() == 2) {
+        nbr[v[0].first * 6 + v[0].second] = (int)v[1].first;
+        nbr[v[1].first * 6 + v[1].second] = (int)v[0].first;
+      }
+    }
+    CUDA_TRY(cudaMemcpy(NT.wts, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(NT.nbr, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice));
+    NT.ready = true;
+  }
+  // seeded initial parameters: Xavier-uniform hidden layers, zero output layer
+  // (the network starts as Jacobi through its skip term)
+  {
+    const int NIN = N + 6, H = NET_H;
+    std::vector<float> p(NT.nparam, 0.f);
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<float> U(-1.f, 1.f);
+    const float a1 = std::sqrt(6.f / (NIN + H)), a2 = std::sqrt(6.f / (H + H));
+    for (int i = 0; i < NIN * H; ++i) p[i] = a1 * U(rng);
+    const int o_w2 = NIN * H + H;
+    for (int i = 0; i < H * H; ++i) p[o_w2 + i] = a2 * U(rng);
+    CUDA_TRY(cudaMemcpy(NT.params, p.data(), p.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(NT.m1, 0, (size_t)NT.nparam * 4));
+    CUDA_TRY(cudaMemset(NT.m2, 0, (size_t)NT.nparam * 4));
+    NT.step = 0;
+  }
+  if (harvest_capacity > 0 && harvest_capacity != NT.cap) {
+    if ((rc = c->alloc(&NT.hr, (size_t)harvest_capacity * c->npoin)) ||
+        (rc = c->alloc(&NT.he, (size_t)harvest_capacity * c->npoin)) ||
+        (rc = c->alloc(&NT.xsnap, (size_t)16 * c->npoin)))
+      return rc;
+    CUDA_TRY(cudaMemset(NT.hr, 0, (size_t)harvest_capacity * c->npoin * 4));
+    CUDA_TRY(cudaMemset(NT.he, 0, (size_t)harvest_capacity * c->npoin * 4));
+    NT.cap = harvest_capacity;
+    NT.count = NT.next = 0;
+    NT.eAe.assign(harvest_capacity, 1.0);
+  }
+  return 0;
+}
+
+int sod_gpu_precond_set_params(sod_gpu_ctx *c, const float *host_params, int n) {
+  if (!c || !c->net.ready || !host_params || n != c->net.nparam) return fail(SOD_GPU_EINVAL, "bad argument");
+  CUDA_TRY(cudaMemcpy(c->net.params, host_params, (size_t)n * 4, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int sod_gpu_precond_get_params(sod_gpu_ctx *c, float *host_params, int n) {
+  if (!c || !c->net.ready || !host_params || n != c->net.nparam) return fail(SOD_GPU_EINVAL, "bad argument");
+  CUDA_TRY(cudaMemcpy(host_params, c->net.params, (size_t)n * 4, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int sod_gpu_precond_apply(sod_gpu_ctx *c, const double *r, double *z) {
+  if (!c || !r || !z) return fail(SOD_GPU_EINVAL, "bad argument");
+  int rc;
+  if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c))) return rc;
+  k_inv_diag64<<<nblk(c->npoin, 256), 256, 0, c->stream>>>((long long)c->npoin, c->cg.diag, c->cg.Minv);
+  if ((rc = apply_precond(c, 1, r, z))) return rc;
+  return c->finish();
+}
+
+int sod_gpu_precond_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double *loss, float *grad_host) {
+  if (!c || !c->net.ready || !r || !e || !loss) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &NT = c->net;
+  k_inv_diag64<<<nblk(c->npoin, 256), 256, 0, c->stream>>>((long long)c->npoin, c->cg.diag, c->cg.Minv);
+  // eAe
+  lap<double>(c, e, NT.tmp2);
+  dots<double, 1>(c, DotArgs<double, 1>{{e}, {NT.tmp2}, {nullptr}}, c->cg.dots + 5);
+  double eAe;
+  CUDA_TRY(cudaMemcpyAsync(&eAe, c->cg.dots + 5, 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (!(eAe > 0)) return fail(SOD_GPU_EINVAL, "target has zero energy norm");
+  int rc = net_loss_grad(c, r, e, eAe, NT.part, loss);
+  if (rc) return rc;
+  k_adam<<<nblk(NT.nparam, 256), 256, 0, c->stream>>>(NT.nparam, NT.nblk_bwd, NT.part, NT.params, NT.m1, NT.m2, 0.f,
+                                                      0.9f, 0.999f, 1e-8f, 1.f, 1.f, 1.f, NT.grad);
+  if (grad_host) CUDA_TRY(cudaMemcpyAsync(grad_host, NT.grad, (size_t)NT.nparam * 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return c->finish();
+}
+
+int sod_gpu_precond_harvest_count(sod_gpu_ctx *c) { return c ? c->net.count : 0; }
+
+// Adam on the harvested (r, e) pairs: `steps` updates of `batch` pairs each;
+// *final_loss (host) = mean relative A-norm loss of the last batch.
+int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64_t seed, float *final_loss) {
+  if (!c || !c->net.ready || steps < 0 || batch < 1 || batch > 16) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &NT = c->net;
+  if (NT.count < 1) return fail(SOD_GPU_EINVAL, "no harvested pairs to train on");
+  k_inv_diag64<<<nblk(c->npoin, 256), 256, 0, c->stream>>>((long long)c->npoin, c->cg.diag, c->cg.Minv);
+  double *rd = c->cg.z1, *ed = c->cg.q;  // FP64 staging of one pair (solver scratch, idle here)
+  std::mt19937_64 rng(seed);
+  double last = 0.0;
+  const int nw = c->npoin_w;
+  const size_t N = c->npoin;
+  for (int st = 0; st < steps; ++st) {
+    double sum = 0.0;
+    for (int b = 0; b < batch; ++b) {
+      const int k = (int)(rng() % (uint64_t)NT.count);
+      k_f2d_w<<<nblk(nw, 256), 256, 0, c->stream>>>(nw, c->lpoin_w, NT.hr + (size_t)k * N, rd);
+      k_f2d_w<<<nblk(nw, 256), 256, 0, c->stream>>>(nw, c->lpoin_w, NT.he + (size_t)k * N, ed);
+      double l = 0.0;
+      int rc = net_loss_grad(c, rd, ed, NT.eAe[k], NT.part + (size_t)b * NT.nblk_bwd * NT.nparam,
+                             (st == steps - 1) ? &l : nullptr);
+      if (rc) return rc;
+      sum += l;
+    }
+    NT.step += 1;
+    const float bc1 = 1.f - std::pow(0.9f, (float)NT.step), bc2 = 1.f - std::pow(0.999f, (float)NT.step);
+    k_adam<<<nblk(NT.nparam, 256), 256, 0, c->stream>>>(NT.nparam, NT.nblk_bwd * batch, NT.part, NT.params, NT.m1,
+                                                        NT.m2, lr, 0.9f, 0.999f, 1e-8f, bc1, bc2, 1.f / batch,
+                                                        nullptr);
+    last = sum / batch;
+  }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (final_loss) *final_loss = (float)last;
+  return c->finish();
+}
+
+}  // extern "C"
+
+// ---- incompressible projection step -------------------------------------
+
+namespace {
+
+// u* = u - dt (R + nu L) * invMl over working nodes (3 components)
+__global__ void k_predictor(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
+                            const float *__restrict__ invMl, const float *__restrict__ u, const float *__restrict__ R,
+                            const float *__restrict__ L, float dt, float nu, float *__restrict__ us) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const long long i = lpoin_w[t];
+  const float im = invMl[i];
+  for (int d = 0; d < 3; ++d) {
+    const long long k = i + npoin * d;
+    us[k] = u[k] - dt * (R[k] + nu * L[k]) * im;
+  }
+}
+
+// b = -div/dt ; x = 2 p - pold (working nodes)
+__global__ void k_poisson_rhs(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ div, float dt,
+                              const double *__restrict__ p, const double *__restrict__ pold, int nhist,
+                              double *__restrict__ b, double *__restrict__ x) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  b[i] = -(double)div[i] / (double)dt;
+  x[i] = nhist >= 2 ? 2.0 * p[i] - pold[i] : (nhist == 1 ? p[i] : 0.0);
+}
+
+// u = u* - dt grad p ; pold = p ; p = x ; pf = (float) x
+__global__ void k_corrector(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
+                            const float *__restrict__ us, const float *__restrict__ gp, float dt,
+                            float *__restrict__ u) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const long long i = lpoin_w[t];
+  for (int d = 0; d < 3; ++d) {
+    const long long k = i + npoin * d;
+    u[k] = us[k] - dt * gp[k];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
+  if (!c || !u || nu < 0) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &I = c->inc;
+  const size_t N = c->npoin;
+  int rc;
+  if (!I.ready) {
+    if ((rc = c->alloc(&I.u, 3 * N)) || (rc = c->alloc(&I.ustar, 3 * N)) || (rc = c->alloc(&I.R, 3 * N)) ||
+        (rc = c->alloc(&I.L, 3 * N)) || (rc = c->alloc(&I.div, N)) || (rc = c->alloc(&I.grad, 3 * N)) ||
+        (rc = c->alloc(&I.pf, N)) || (rc = c->alloc(&I.p, N)) || (rc = c->alloc(&I.pold, N)) ||
+        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)))
+      return rc;
+    I.ready = true;
+  }
+  CUDA_TRY(cudaMemcpyAsync(I.u, u, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  for (float *z : {I.ustar, I.R, I.L, I.grad}) CUDA_TRY(cudaMemsetAsync(z, 0, 3 * N * 4, c->stream));
+  for (double *z : {I.p, I.pold, I.b, I.x}) CUDA_TRY(cudaMemsetAsync(z, 0, N * 8, c->stream));
+  CUDA_TRY(cudaMemsetAsync(I.div, 0, N * 4, c->stream));
+  CUDA_TRY(cudaMemsetAsync(I.pf, 0, N * 4, c->stream));
+  I.nu = nu;
+  I.nsteps = 0;
+  return c->finish();
+}
+
+int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats) {
+  if (!c || !c->inc.ready || !opts || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &I = c->inc;
+  const long long N = c->npoin;
+  const int nw = c->npoin_w;
+  const unsigned nb = nblk(nw, 256);
+  const bool was_async = c->async;
+  c->async = true;  // chain the operator calls; synchronise at the end
+  int rc = sod_gpu_full_convec_ijk_incomp(c, I.u, I.u, I.R);
+  for (int d = 0; d < 3 && !rc; ++d) {
+    CUDA_TRY(cudaMemsetAsync(I.L + N * d, 0, N * 4, c->stream));
+    lap<float>(c, I.u + N * d, I.L + N * d);
+  }
+  if (rc) { c->async = was_async; return rc; }
+  k_predictor<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->invMl, I.u, I.R, I.L, dt, (float)I.nu, I.ustar);
+  rc = sod_gpu_eval_divergence(c, I.ustar, I.div);
+  if (rc) { c->async = was_async; return rc; }
+  k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, dt, I.p, I.pold, I.nsteps, I.b, I.x);
+  c->async = was_async;
+  rc = sod_gpu_pressure_solve(c, I.b, I.x, opts, stats);
+  if (rc && rc != SOD_GPU_ESTAGNATE) return rc;
+  const int solve_rc = rc;
+  c->async = true;
+  CUDA_TRY(cudaMemcpyAsync(I.pold, I.p, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(I.p, I.x, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  k_d2f_w<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.p, I.pf);
+  rc = sod_gpu_eval_gradient(c, I.pf, I.grad);
+  c->async = was_async;
+  if (rc) return rc;
+  k_corrector<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, I.ustar, I.grad, dt, I.u);
+  I.nsteps++;
+  rc = c->finish();
+  return rc ? rc : solve_rc;
+}
+
+int sod_gpu_incomp_get(sod_gpu_ctx *c, float *u, double *p) {
+  if (!c || !c->inc.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
+  if (u) CUDA_TRY(cudaMemcpyAsync(u, c->inc.u, (size_t)c->npoin * 12, cudaMemcpyDeviceToDevice, c->stream));
+  if (p) CUDA_TRY(cudaMemcpyAsync(p, c->inc.p, (size_t)c->npoin * 8, cudaMemcpyDeviceToDevice, c->stream));
   return c->finish();
 }
 

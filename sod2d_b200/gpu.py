@@ -28,7 +28,8 @@ class SodMesh(C.Structure):
 
 
 class SolveOpts(C.Structure):
-    _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("precond", C.c_int), ("stagnation_window", C.c_int)]
+    _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("precond", C.c_int), ("stagnation_window", C.c_int),
+                ("harvest", C.c_int)]
 
 
 class SolveStats(C.Structure):
@@ -75,6 +76,17 @@ SIGNATURES = {
     "sod_gpu_conjgrad_pressure": (C.c_int, [VP, VP, VP, C.c_int, C.c_double, C.POINTER(C.c_int),
                                             C.POINTER(C.c_double)]),
     "sod_gpu_pressure_solve": (C.c_int, [VP, VP, VP, VP, VP]),
+    "sod_gpu_precond_num_params": (C.c_int, [VP]),
+    "sod_gpu_precond_init": (C.c_int, [VP, C.c_uint64, C.c_int]),
+    "sod_gpu_precond_set_params": (C.c_int, [VP, VP, C.c_int]),
+    "sod_gpu_precond_get_params": (C.c_int, [VP, VP, C.c_int]),
+    "sod_gpu_precond_apply": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_precond_loss_grad": (C.c_int, [VP, VP, VP, C.POINTER(C.c_double), VP]),
+    "sod_gpu_precond_harvest_count": (C.c_int, [VP]),
+    "sod_gpu_precond_train": (C.c_int, [VP, C.c_int, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "sod_gpu_incomp_init": (C.c_int, [VP, VP, C.c_double]),
+    "sod_gpu_incomp_step": (C.c_int, [VP, C.c_float, VP, VP]),
+    "sod_gpu_incomp_get": (C.c_int, [VP, VP, VP]),
     "sod_gpu_analysis_noalloc": (C.c_int, [C.c_int] * 4 + [VP] * 15 + [C.c_float, C.c_float, VP,
                                                                        C.POINTER(C.c_double)]),
 }

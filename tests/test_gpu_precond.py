@@ -1,0 +1,107 @@
+"""Learned preconditioner on the GPU: forward/backward kernels against the
+numpy restatement, and the gain of the trained network over Jacobi inside
+the FP64-certified flexible CG on pressure systems of an incompressible
+Taylor-Green run."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+import precond_ref as PR
+from sod2d_b200 import host
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from sod2d_b200 import gpu as g
+    return g
+
+
+def test_loss_and_gradient_match_oracle(gpu):
+    m = host.periodic_cube(3, 4, jitter=0.05, seed=6, ordering=1, elem_shuffle=True)
+    ctx = gpu.Context(m, gpu.default_phys())
+    ctx.call("sod_gpu_precond_init", 7, 0)
+    n = gpu.lib().sod_gpu_precond_num_params(ctx.h)
+    rng = np.random.default_rng(3)
+    params = rng.normal(0, 0.2, n).astype(np.float32)
+    ctx.call("sod_gpu_precond_set_params", params.ctypes.data_as(C.c_void_p), n)
+    om = O.OracleMesh(m, np.float64)
+    diag = torch.zeros(m.npoin, device="cuda")
+    ctx.call("sod_gpu_eval_laplacian_diag", gpu.dptr(diag))
+    w = m.lpoin_w - 1
+    Minv = np.zeros(m.npoin)
+    Minv[w] = 1.0 / diag.cpu().numpy()[w].astype(np.float64)
+    net = PR.Net(m, Minv)
+    e = np.zeros(m.npoin)
+    e[w] = rng.normal(size=w.size)
+    r = O.laplacian(om, e)
+    ref_loss, ref_grad = net.loss_grad(params.astype(np.float64), r, e, lambda v: O.laplacian(om, v))
+    loss = C.c_double()
+    grad = np.zeros(n, np.float32)
+    dr, de = torch.from_numpy(r).cuda(), torch.from_numpy(e).cuda()
+    ctx.call("sod_gpu_precond_loss_grad", gpu.dptr(dr), gpu.dptr(de), C.byref(loss), grad.ctypes.data_as(C.c_void_p))
+    print("loss", loss.value, ref_loss)
+    assert abs(loss.value - ref_loss) / ref_loss < 1e-4
+    err = np.linalg.norm(grad - ref_grad) / np.linalg.norm(ref_grad)
+    print("grad rel L2", err)
+    assert err < 1e-3
+    # forward: apply == oracle forward
+    z = torch.zeros(m.npoin, dtype=torch.float64, device="cuda")
+    ctx.call("sod_gpu_precond_apply", gpu.dptr(dr), gpu.dptr(z))
+    zr, _ = net.forward(params.astype(np.float64), r)
+    assert np.linalg.norm(z.cpu().numpy()[w] - zr[w]) / np.linalg.norm(zr[w]) < 1e-5
+    ctx.close()
+
+
+def test_trained_network_beats_jacobi(gpu):
+    m = host.periodic_cube(3, 8)
+    N = m.npoin
+    x, y, z = (m.coord[i * N:(i + 1) * N].astype(np.float64) for i in range(3))
+    u = np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),
+                        np.zeros(N)]).astype(np.float32)
+    ctx = gpu.Context(m, gpu.default_phys())
+    ctx.call("sod_gpu_precond_init", 11, 48)
+    du = torch.from_numpy(u).cuda()
+    ctx.call("sod_gpu_incomp_init", gpu.dptr(du), 1.0 / 1600.0)
+    dt = 0.02
+    jac = gpu.SolveOpts(20000, 1e-8, 0, 100, 1)
+    st = gpu.SolveStats()
+    its_j = []
+    for k in range(12):  # Jacobi steps, harvesting
+        ctx.call("sod_gpu_incomp_step", dt, C.byref(jac), C.byref(st))
+        its_j.append(st.iterations)
+        assert st.res_rel < 1e-8
+    assert gpu.lib().sod_gpu_precond_harvest_count(ctx.h) > 10
+    loss = C.c_float()
+    ctx.call("sod_gpu_precond_train", 300, 8, 2e-3, 5, C.byref(loss))
+    print("Jacobi iterations", its_j, "final training loss", loss.value)
+    # the next pressure system, solved from the same zero initial guess by both
+    uu = torch.zeros(3 * N, device="cuda")
+    ctx.call("sod_gpu_incomp_get", gpu.dptr(uu), None)
+    R = torch.zeros(3 * N, device="cuda")
+    ctx.call("sod_gpu_full_convec_ijk_incomp", gpu.dptr(uu), gpu.dptr(uu), gpu.dptr(R))
+    L = torch.zeros(3 * N, device="cuda")
+    for d in range(3):
+        ctx.call("sod_gpu_eval_laplacian_mult", gpu.dptr(uu[d * N:]), gpu.dptr(L[d * N:]))
+    invMl = torch.from_numpy(m.invMl).cuda().repeat(3)
+    us = uu - dt * (R + (1.0 / 1600.0) * L) * invMl
+    div = torch.zeros(N, device="cuda")
+    ctx.call("sod_gpu_eval_divergence", gpu.dptr(us), gpu.dptr(div))
+    b = (-div.double() / dt).contiguous()
+    out = {}
+    for name, kind in (("jacobi", 0), ("learned", 1)):
+        x0 = torch.zeros(N, dtype=torch.float64, device="cuda")
+        o = gpu.SolveOpts(20000, 1e-8, kind, 200, 0)
+        st = gpu.SolveStats()
+        ctx.call("sod_gpu_pressure_solve", gpu.dptr(b), gpu.dptr(x0), C.byref(o), C.byref(st))
+        out[name] = (st.iterations, st.res_rel, st.fallback, st.seconds)
+    print("jacobi:", out["jacobi"], " learned:", out["learned"])
+    assert out["learned"][1] < 1e-8 and out["learned"][2] == 0
+    assert out["learned"][0] < out["jacobi"][0]
+    ctx.close()
