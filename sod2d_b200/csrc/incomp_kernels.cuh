@@ -123,7 +123,7 @@ k_vec_elem(MeshDev m, const float *__restrict__ x, const float *__restrict__ u, 
            float *__restrict__ slots) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
   constexpr int NF = MODE == 0 ? 1 : (MODE == 1 ? 3 : 12);
-  __shared__ float sm[EPB][NF][N];
+  __shared__ __align__(16) float sm[EPB][NF][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
   const long long e = (long long)blockIdx.x * EPB + el;
   const bool active = (e < m.nelem) && (t < N);

@@ -15,6 +15,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#ifndef SOD_VEC_XI
+#define SOD_VEC_XI 1
+#endif
+#ifndef SOD_RHS_MINB
+#define SOD_RHS_MINB 6
+#endif
+
 namespace sod {
 
 template <int P>
@@ -58,6 +65,21 @@ __device__ __forceinline__ void iso_grad(const float *__restrict__ f, int i, int
                                          const float (&Dk)[P + 1], float &g0, float &g1, float &g2) {
   constexpr int N1 = P + 1;
   g0 = 0.f; g1 = 0.f; g2 = 0.f;
+#if SOD_VEC_XI
+  if constexpr (P == 3) {
+    // the xi-line of a 4-node element row is one aligned 16-byte load
+    const float4 v = *reinterpret_cast<const float4 *>(f + 4 * j + 16 * k);
+    const float fx[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int s = 0; s < N1; ++s) {
+      const int m = ref_order<P>(s);
+      g0 = fmaf(Di[m], fx[m], g0);
+      g1 = fmaf(Dj[m], f[i + N1 * m + N1 * N1 * k], g1);
+      g2 = fmaf(Dk[m], f[i + N1 * j + N1 * N1 * m], g2);
+    }
+    return;
+  }
+#endif
 #pragma unroll
   for (int s = 0; s < N1; ++s) {
     const int m = ref_order<P>(s);
@@ -90,8 +112,10 @@ __device__ __forceinline__ void eos(const Phys &ph, float Rgas, float mu_factor,
 
 // ---------------------------------------------------------------------
 // Pass A: LPS projections (full_proj_ijk, elem_stab.f90:474-562).  Writes
-// gpvol * {tau row x (3), tau row y (3), tau row z (3), grad rho (3),
-// grad T (3)} per element node into slots of width 16.
+// gpvol * {tau00, tau01, tau02, tau11, tau12, tau22, grad rho (3), grad T
+// (3)} per element node into slots of width 12.  tau = grad u + grad u^T
+// - 2/3 div u I is symmetric (tau_ab and tau_ba are the same FP32 sum), so
+// the reference's ProjMX/MY/MZ rows are read back from its 6 entries.
 // Input: conserved state (SoA, reference layout) -> EOS in registers, or
 // primitive rho/u/T (prim = true).
 // ---------------------------------------------------------------------
@@ -100,7 +124,7 @@ __global__ void __launch_bounds__(EPB *Cfg<P>::NT)
 k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float *__restrict__ a1,
        const float *__restrict__ a2, float *__restrict__ slots) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT, NF = 5;
-  __shared__ float sm[EPB][NF][N];
+  __shared__ __align__(16) float sm[EPB][NF][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
   const long long e = (long long)blockIdx.x * EPB + el;
   const bool active = (e < m.nelem) && (t < N);
@@ -145,7 +169,7 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
 #pragma unroll
     for (int b = 0; b < 3; ++b) gradU[a][b] = He[b] * gU[a][0] + He[b + 3] * gU[a][1] + He[b + 6] * gU[a][2];
   const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
-  float4 *o = reinterpret_cast<float4 *>(slots + (e * N + t) * 16);
+  float4 *o = reinterpret_cast<float4 *>(slots + (e * N + t) * 12);
   float tau[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -153,10 +177,9 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
     for (int b = 0; b < 3; ++b) tau[a][b] = gradU[a][b] + gradU[b][a];
     tau[a][a] = tau[a][a] - ph.twoThirds * divU;
   }
-  o[0] = make_float4(gv * tau[0][0], gv * tau[0][1], gv * tau[0][2], gv * tau[1][0]);
-  o[1] = make_float4(gv * tau[1][1], gv * tau[1][2], gv * tau[2][0], gv * tau[2][1]);
-  o[2] = make_float4(gv * tau[2][2], gv * gradRho[0], gv * gradRho[1], gv * gradRho[2]);
-  o[3] = make_float4(gv * gradT[0], gv * gradT[1], gv * gradT[2], 0.f);
+  o[0] = make_float4(gv * tau[0][0], gv * tau[0][1], gv * tau[0][2], gv * tau[1][1]);
+  o[1] = make_float4(gv * tau[1][2], gv * tau[2][2], gv * gradRho[0], gv * gradRho[1]);
+  o[2] = make_float4(gv * gradRho[2], gv * gradT[0], gv * gradT[1], gv * gradT[2]);
 }
 
 // ---------------------------------------------------------------------
@@ -182,7 +205,8 @@ struct RhsArgs {
   const float *mue_t;     // [nelem][N] tensor order (internal copy of mu_e)
   const float *musgs_t;   // [nelem][N] or null
   const float *tau_stab;  // (nelem)
-  const float *proj16;    // [npoin][16] mass-inverted projections (internal)
+  const float *proj12;    // [npoin][12] mass-inverted projections (internal):
+                          // tau00 tau01 tau02 tau11 tau12 tau22 gradRho(3) gradT(3)
   float fact_c, fact_d;
 };
 
@@ -202,12 +226,12 @@ __device__ __forceinline__ int sym_idx(int a, int b) {
 }
 
 template <int P, int EPB, int MODE, int IN>
-__global__ void __launch_bounds__(EPB *Cfg<P>::NT)
+__global__ void __launch_bounds__(EPB *Cfg<P>::NT, SOD_RHS_MINB)
 k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
   constexpr bool CONV = (MODE & MODE_CONV) != 0;
   constexpr bool DIFF = (MODE & MODE_DIFF) != 0;
-  __shared__ float sm[EPB][NF_B][N];
+  __shared__ __align__(16) float sm[EPB][NF_B][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
   const long long e = (long long)blockIdx.x * EPB + el;
   const bool active = (e < m.nelem) && (t < N);
@@ -379,10 +403,10 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
         for (int b = 0; b < 3; ++b) tau[a][b] = gradU[a][b] + gradU[b][a];
         tau[a][a] = tau[a][a] - ph.twoThirds * divU;
       }
-      const float4 *pj = reinterpret_cast<const float4 *>(A.proj16 + (long long)node * 16);
-      const float4 p0 = pj[0], p1 = pj[1], p2 = pj[2], p3 = pj[3];
-      const float PX[3] = {p0.x, p0.y, p0.z}, PY[3] = {p0.w, p1.x, p1.y}, PZ[3] = {p1.z, p1.w, p2.x};
-      const float PM[3] = {p2.y, p2.z, p2.w}, PE[3] = {p3.x, p3.y, p3.z};
+      const float4 *pj = reinterpret_cast<const float4 *>(A.proj12 + (long long)node * 12);
+      const float4 p0 = pj[0], p1 = pj[1], p2 = pj[2];
+      const float PX[3] = {p0.x, p0.y, p0.z}, PY[3] = {p0.y, p0.w, p1.x}, PZ[3] = {p0.z, p1.x, p1.y};
+      const float PM[3] = {p1.z, p1.w, p2.x}, PE[3] = {p2.y, p2.z, p2.w};
       const float u[3] = {s.u0, s.u1, s.u2};
       float Fx[3], Fy[3], Fz[3], FT[3], FR[3];
       const float cl = -ph.c_lps * ts;
@@ -463,14 +487,14 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
 // Node-centric assembly: out_f(p) = scale(p) * (base_f(p) + sum of the
 // node's slot contributions), Kahan-compensated, slots visited in element
 // order (deterministic).  W = slot width, NFO = fields summed.
-// Output layout: SoA (reference, out[f][p] = out + f*npoin) when AOS16 is
-// false; node-major [p][16] when true.
+// Output layout: SoA (reference, out[f][p] = out + f*npoin) when AOS is
+// false; node-major [p][W] when true.
 // ---------------------------------------------------------------------
 struct OutPtrs {
   float *p[16];
 };
 
-template <int W, int NFO, bool AOS16>
+template <int W, int NFO, bool AOS>
 __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__restrict__ out,
                          OutPtrs out_soa, int accumulate, int use_invMl) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -478,7 +502,7 @@ __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__re
   float sum[NFO], cmp[NFO];
 #pragma unroll
   for (int f = 0; f < NFO; ++f) {
-    sum[f] = (accumulate && !AOS16) ? out_soa.p[f][p] : 0.f;
+    sum[f] = (accumulate && !AOS) ? out_soa.p[f][p] : 0.f;
     cmp[f] = 0.f;
   }
   const int b = m.slot_ptr[p], en = m.slot_ptr[p + 1];
@@ -499,13 +523,13 @@ __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__re
     }
   }
   const float sc = use_invMl ? m.invMl[p] : 1.f;
-  if (AOS16) {
-    float4 *o = reinterpret_cast<float4 *>(out + p * 16);
-    float r[16];
+  if (AOS) {
+    float4 *o = reinterpret_cast<float4 *>(out + p * W);
+    float r[W];
 #pragma unroll
-    for (int f = 0; f < 16; ++f) r[f] = f < NFO ? sum[f] * sc : 0.f;
+    for (int f = 0; f < W; ++f) r[f] = f < NFO ? sum[f] * sc : 0.f;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) o[c] = make_float4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+    for (int c = 0; c < W / 4; ++c) o[c] = make_float4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
   } else {
 #pragma unroll
     for (int f = 0; f < NFO; ++f) out_soa.p[f][p] = sum[f] * sc;

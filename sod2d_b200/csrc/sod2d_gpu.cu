@@ -56,7 +56,7 @@ struct sod_gpu_ctx {
   int *a_of_t = nullptr;  // tensor position -> reference local node (0-based)
   float *geo = nullptr, *Dnat = nullptr, *invMl = nullptr, *Ml = nullptr, *helem = nullptr, *helem_l_t = nullptr;
   // scratch
-  float *slotsA = nullptr, *slotsB = nullptr, *proj16 = nullptr, *mue_t = nullptr, *musgs_t = nullptr;
+  float *slotsA = nullptr, *slotsB = nullptr, *proj12 = nullptr, *mue_t = nullptr, *musgs_t = nullptr;
   size_t bytes = 0;
   std::vector<void *> allocs;
   // analysis / entropy-viscosity support
@@ -70,6 +70,7 @@ struct sod_gpu_ctx {
     float *x32, *r32, *p32, *q32, *z032, *z132, *b32;          // reference-arithmetic CG
     double *x, *r, *p, *q, *z0, *z1, *b, *Minv;                // FP64 CG
     double *part, *dots;                                        // reductions
+    double *Pm = nullptr, *Qm = nullptr;                        // truncated-FCG direction ring (7 x npoin each)
   } cg;
   // learned preconditioner
   struct Net {
@@ -172,18 +173,30 @@ __global__ void k_t_to_elem(long long nelem, int N, const int *__restrict__ a_of
   dst[e + nelem * a_of_t[t]] = src[idx];
 }
 
-// Five Proj arrays (npoin,3) -> node-major [p][16].
+// Five Proj arrays (npoin,3) -> node-major [p][12] (tau00 tau01 tau02
+// tau11 tau12 tau22 gradRho gradT); the symmetric stress rows ProjMY(:,1),
+// ProjMZ(:,1:2) equal ProjMX(:,2:3), ProjMY(:,3).
 __global__ void k_pack_proj(long long npoin, const float *PMX, const float *PMY, const float *PMZ,
-                            const float *PMass, const float *PEner, float *proj16) {
+                            const float *PMass, const float *PEner, float *proj12) {
   long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoin) return;
-  const float *src[5] = {PMX, PMY, PMZ, PMass, PEner};
-  float r[16];
-  for (int f = 0; f < 5; ++f)
-    for (int d = 0; d < 3; ++d) r[f * 3 + d] = src[f][p + npoin * d];
-  r[15] = 0.f;
-  float4 *o = reinterpret_cast<float4 *>(proj16 + p * 16);
-  for (int c = 0; c < 4; ++c) o[c] = make_float4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+  const float r[12] = {PMX[p], PMX[p + npoin], PMX[p + 2 * npoin], PMY[p + npoin], PMY[p + 2 * npoin],
+                       PMZ[p + 2 * npoin], PMass[p], PMass[p + npoin], PMass[p + 2 * npoin],
+                       PEner[p], PEner[p + npoin], PEner[p + 2 * npoin]};
+  float4 *o = reinterpret_cast<float4 *>(proj12 + p * 12);
+  for (int c = 0; c < 3; ++c) o[c] = make_float4(r[4 * c], r[4 * c + 1], r[4 * c + 2], r[4 * c + 3]);
+}
+
+__global__ void k_unpack_proj(long long npoin, const float *proj12, float *PMX, float *PMY, float *PMZ,
+                              float *PMass, float *PEner) {
+  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npoin) return;
+  const float *r = proj12 + p * 12;
+  PMX[p] = r[0]; PMX[p + npoin] = r[1]; PMX[p + 2 * npoin] = r[2];
+  PMY[p] = r[1]; PMY[p + npoin] = r[3]; PMY[p + 2 * npoin] = r[4];
+  PMZ[p] = r[2]; PMZ[p + npoin] = r[4]; PMZ[p + 2 * npoin] = r[5];
+  PMass[p] = r[6]; PMass[p + npoin] = r[7]; PMass[p + 2 * npoin] = r[8];
+  PEner[p] = r[9]; PEner[p + npoin] = r[10]; PEner[p + 2 * npoin] = r[11];
 }
 
 // Primitive outputs of updateF at working nodes (time_integ_ls.f90:574-587).
@@ -252,7 +265,7 @@ int dispatch(sod_gpu_ctx *c, F &&f) {
 
 void gather_proj_aos(sod_gpu_ctx *c) {
   OutPtrs none{};
-  k_gather<16, 15, true><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsA, c->proj16, none, 0, 1);
+  k_gather<12, 12, true><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsA, c->proj12, none, 0, 1);
 }
 
 void gather_res(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener, int accumulate, int invml) {
@@ -341,8 +354,8 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
       (rc = c->upload(&c->slot_idx, slot_idx.data(), slot_idx.size())) ||
       (rc = c->upload(&c->invMl, mesh->invMl, (size_t)NP)) || (rc = c->upload(&c->Ml, mesh->Ml, (size_t)NP)) ||
       (rc = c->upload(&c->a_of_t, a_of_t.data(), a_of_t.size())) ||
-      (rc = c->alloc(&c->slotsA, (size_t)E * N * 16)) || (rc = c->alloc(&c->slotsB, (size_t)E * N * 8)) ||
-      (rc = c->alloc(&c->proj16, (size_t)NP * 16)) || (rc = c->alloc(&c->mue_t, (size_t)E * N))) {
+      (rc = c->alloc(&c->slotsA, (size_t)E * N * 12)) || (rc = c->alloc(&c->slotsB, (size_t)E * N * 8)) ||
+      (rc = c->alloc(&c->proj12, (size_t)NP * 12)) || (rc = c->alloc(&c->mue_t, (size_t)E * N))) {
     sod_gpu_finalize(c);
     return rc;
   }
@@ -436,12 +449,11 @@ int sod_gpu_full_proj_ijk(sod_gpu_ctx *c, const float *rho, const float *u, cons
     return 0;
   });
   if (rc) return rc;
-  OutPtrs o{};
-  const long long N = c->npoin;
-  float *f5[5] = {ProjMX, ProjMY, ProjMZ, ProjMass, ProjEner};
-  for (int f = 0; f < 5; ++f)
-    for (int d = 0; d < 3; ++d) o.p[f * 3 + d] = f5[f] + N * d;
-  k_gather<16, 15, false><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsA, nullptr, o, 0, 1);
+  // assemble into the node-major 12-wide buffer, then expand to the
+  // reference's five (npoin,3) arrays
+  gather_proj_aos(c);
+  k_unpack_proj<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, c->proj12, ProjMX, ProjMY, ProjMZ, ProjMass,
+                                                            ProjEner);
   return c->finish();
 }
 
@@ -465,10 +477,10 @@ int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
     k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
   }
   k_pack_proj<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, ProjMX, ProjMY, ProjMZ, ProjMass, ProjEner,
-                                                          c->proj16);
+                                                          c->proj12);
   RhsArgs A{};
   A.rho = rho; A.u = u; A.Tem = Tem; A.mu_fluid = mu_fluid;
-  A.mue_t = c->mue_t; A.musgs_t = mu_sgs ? c->musgs_t : nullptr; A.tau_stab = tau_stab; A.proj16 = c->proj16;
+  A.mue_t = c->mue_t; A.musgs_t = mu_sgs ? c->musgs_t : nullptr; A.tau_stab = tau_stab; A.proj12 = c->proj12;
   A.fact_d = fact;
   Phys saved = c->ph;
   c->ph.Cp = Cp; c->ph.Prt = Pr;
@@ -500,7 +512,7 @@ int sod_gpu_updateF(sod_gpu_ctx *c, const float *rho, const float *q, const floa
   if (mu_e) k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   RhsArgs A{};
   A.rho = rho; A.q = q; A.E = E; A.mu_factor = mu_factor;
-  A.mue_t = c->mue_t; A.tau_stab = tau_stab; A.proj16 = c->proj16;
+  A.mue_t = c->mue_t; A.tau_stab = tau_stab; A.proj12 = c->proj12;
   A.fact_c = -1.0f; A.fact_d = -1.0f;
   int rc = dispatch(c, [&](auto L) {
     L.proj(c, false, rho, q, E);
@@ -589,7 +601,7 @@ int ensure_diag(sod_gpu_ctx *c) {
   if (G.have_diag) return 0;
   int rc;
   if (!G.diag && (rc = c->alloc(&G.diag, (size_t)c->npoin))) return rc;
-  if (!G.part && ((rc = c->alloc(&G.part, 3 * DOT_BLOCKS)) || (rc = c->alloc(&G.dots, 8)))) return rc;
+  if (!G.part && ((rc = c->alloc(&G.part, 8 * DOT_BLOCKS)) || (rc = c->alloc(&G.dots, 16)))) return rc;
   const long long EN = (long long)c->nelem * c->N;
   dispatch(c, [&](auto L) {
     using LL = decltype(L);
@@ -804,6 +816,23 @@ __global__ void k_jacobi64(int npoin_w, const int *__restrict__ lpoin_w, const d
   z[i] = r[i] * Minv[i];
 }
 
+struct MultiAxpy {
+  int n;
+  const double *v[8];
+  double c[8];
+};
+
+// p = z + sum_j c_j v_j over working nodes
+__global__ void k_multi_axpy(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ z, MultiAxpy M,
+                             double *__restrict__ p) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  double a = z[i];
+  for (int j = 0; j < M.n; ++j) a += M.c[j] * M.v[j][i];
+  p[i] = a;
+}
+
 // r = b - q over working nodes
 __global__ void k_resid(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ b,
                         const double *__restrict__ q, double *__restrict__ r) {
@@ -851,7 +880,7 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
   int next_snap = 0;
   auto take_snapshot = [&](int iter_no) {
     if (!harvest || (int)snaps.size() >= 16 || iter_no != next_snap) return;
-    next_snap = next_snap == 0 ? 1 : next_snap * 2;
+    next_snap = next_snap < 8 ? next_snap + 1 : next_snap * 2;
     const int slot = NT.next;
     NT.next = (NT.next + 1) % NT.cap;
     if (NT.count < NT.cap) NT.count++;
@@ -862,7 +891,7 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
   };
   if (bnorm == 0.0) {
     CUDA_TRY(cudaMemsetAsync(x, 0, N * 8, st));
-  } else {
+  } else if (kind == 0) {
     bool converged = false;
     while (!converged && it < opts->max_iter) {
       // (re)start: r = b - A x (FP64 true residual), z = M r, p = z
@@ -908,6 +937,93 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
         res = nrm;
         take_snapshot(it);
       }
+    }
+  } else {
+    // truncated flexible CG with the learned preconditioner
+    const int m = opts->truncation > 0 ? (opts->truncation < 7 ? opts->truncation : 7) : 4;
+    if (!G.Pm && ((rc = c->alloc(&G.Pm, 7 * N)) || (rc = c->alloc(&G.Qm, 7 * N)))) return rc;
+    double pAp[7];
+    bool converged = false;
+    while (!converged && it < opts->max_iter) {
+      lap<double>(c, x, G.q);
+      k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
+      int nd = 0;  // stored directions
+      double best = 1e300;
+      int best_it = it;
+      bool restart = false;
+      while (!restart && it < opts->max_iter) {
+        if ((rc = apply_precond(c, kind, G.r, G.z0))) return rc;
+        // dots: ||r||^2 and z.Q_j for the stored directions (one pass)
+        const int nq = nd < m ? nd : m;
+        DotArgs<double, 8> A8{};
+        A8.a[0] = G.r; A8.b[0] = G.r; A8.c[0] = nullptr;
+        for (int j = 0; j < 7; ++j) {
+          A8.a[1 + j] = G.z0;
+          A8.b[1 + j] = (j < nq) ? G.Qm + (size_t)j * N : G.r;
+          A8.c[1 + j] = nullptr;
+        }
+        dots<double, 8>(c, A8, G.dots + 8);
+        double hd[8];
+        CUDA_TRY(cudaMemcpyAsync(hd, G.dots + 8, 64, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        const double nrm = std::sqrt(hd[0]) / bnorm;
+        if (!std::isfinite(nrm)) return fail(SOD_GPU_ENONFINITE, "non-finite residual in pressure solve");
+        res = nrm;
+        if (nrm < best * 0.5) { best = nrm; best_it = it; }
+        if (nrm < opts->tol) {
+          lap<double>(c, x, G.q);
+          k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
+          dots<double, 1>(c, DotArgs<double, 1>{{G.r}, {G.r}, {nullptr}}, G.dots + 2);
+          double h1;
+          CUDA_TRY(cudaMemcpyAsync(&h1, G.dots + 2, 8, cudaMemcpyDeviceToHost, st));
+          CUDA_TRY(cudaStreamSynchronize(st));
+          res = std::sqrt(h1) / bnorm;
+          if (res < opts->tol) converged = true;
+          restart = true;
+          break;
+        }
+        if (it - best_it > window) {  // stagnation: fall back to Jacobi
+          kind = 0;
+          fallback = 1;
+          break;
+        }
+        // p = z - sum_j (z.Q_j / pAp_j) P_j   (A-orthogonal to the stored directions)
+        const int slot = nd % m;
+        MultiAxpy MA{};
+        MA.n = nq;
+        for (int j = 0; j < nq; ++j) {
+          MA.v[j] = G.Pm + (size_t)j * N;
+          MA.c[j] = -(hd[1 + j] / pAp[j]);
+        }
+        double *pnew = G.Pm + (size_t)slot * N, *qnew = G.Qm + (size_t)slot * N;
+        k_multi_axpy<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.z0, MA, G.p);
+        CUDA_TRY(cudaMemcpyAsync(pnew, G.p, N * 8, cudaMemcpyDeviceToDevice, st));
+        lap<double>(c, pnew, qnew);
+        dots<double, 2>(c, DotArgs<double, 2>{{pnew, pnew}, {qnew, G.r}, {nullptr, nullptr}}, G.dots + 2);
+        double ha[2];
+        CUDA_TRY(cudaMemcpyAsync(ha, G.dots + 2, 16, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        if (!(ha[0] > 0.0)) { restart = true; break; }  // lost positivity: restart from the true residual
+        pAp[slot] = ha[0];
+        const double alpha = ha[1] / ha[0];
+        k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, alpha, pnew, 1.0, x);
+        k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, -alpha, qnew, 1.0, G.r);
+        ++nd;
+        ++it;
+      }
+      if (kind == 0 && fallback) break;
+    }
+    if (fallback && !converged) {
+      // continue with Jacobi CG from the current iterate
+      sod_solve_opts_t o2 = *opts;
+      o2.precond = 0;
+      o2.harvest = 0;
+      o2.max_iter = opts->max_iter - it > 1 ? opts->max_iter - it : 1;
+      sod_solve_stats_t s2{};
+      int rc2 = sod_gpu_pressure_solve(c, b_in, x, &o2, &s2);
+      it += s2.iterations;
+      res = s2.res_rel;
+      if (rc2 && rc2 != SOD_GPU_ESTAGNATE) return rc2;
     }
   }
   // harvested pairs: e_k = x* - x_k and their energy norms
@@ -1031,7 +1147,7 @@ void comp_updateF(sod_gpu_ctx *c) {
   auto &S = c->comp;
   RhsArgs A{};
   A.rho = S.rho32; A.q = S.q32; A.E = S.E32; A.mu_factor = S.mu_factor;
-  A.mue_t = c->mue_t; A.tau_stab = S.tau; A.proj16 = c->proj16;
+  A.mue_t = c->mue_t; A.tau_stab = S.tau; A.proj12 = c->proj12;
   A.fact_c = -1.0f; A.fact_d = -1.0f;
   dispatch(c, [&](auto L) {
     L.proj(c, false, S.rho32, S.q32, S.E32);
@@ -1626,7 +1742,11 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
   k_predictor<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->invMl, I.u, I.R, I.L, dt, (float)I.nu, I.ustar);
   rc = sod_gpu_eval_divergence(c, I.ustar, I.div);
   if (rc) { c->async = was_async; return rc; }
-  k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, dt, I.p, I.pold, I.nsteps, I.b, I.x);
+  // initial guess: the previous pressure for Jacobi (the reference's x0,
+  // mod_solver_incomp.f90:306); extrapolated from the previous two
+  // pressures for the learned path
+  const int hist = opts->precond == 1 ? I.nsteps : (I.nsteps > 0 ? 1 : 0);
+  k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, dt, I.p, I.pold, hist, I.b, I.x);
   c->async = was_async;
   rc = sod_gpu_pressure_solve(c, I.b, I.x, opts, stats);
   if (rc && rc != SOD_GPU_ESTAGNATE) return rc;

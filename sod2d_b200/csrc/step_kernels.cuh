@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(EPB *Cfg<P>::NT)
 k_entropy_elem(MeshDev m, const float *__restrict__ feta, const float *__restrict__ eta1,
                const float *__restrict__ u1, const float *__restrict__ u2, float *__restrict__ slots) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT, NF = 10;
-  __shared__ float sm[EPB][NF][N];
+  __shared__ __align__(16) float sm[EPB][NF][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
   const long long e = (long long)blockIdx.x * EPB + el;
   const bool active = (e < m.nelem) && (t < N);
@@ -329,7 +329,7 @@ k_analysis_elem(MeshDev m, const float *__restrict__ rho, const float *__restric
                 const float *__restrict__ mu_fluid, const float *__restrict__ mue_t,
                 const float *__restrict__ Ngp_t /*[g][a] tensor order*/, float *__restrict__ part) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
-  __shared__ float sm[EPB][4][N];
+  __shared__ __align__(16) float sm[EPB][4][N];
   __shared__ float red[EPB][3][NT / 32];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT, lane = threadIdx.x % 32, w = t / 32;
   const long long e = (long long)blockIdx.x * EPB + el;

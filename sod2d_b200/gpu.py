@@ -29,7 +29,7 @@ class SodMesh(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("precond", C.c_int), ("stagnation_window", C.c_int),
-                ("harvest", C.c_int)]
+                ("harvest", C.c_int), ("truncation", C.c_int)]
 
 
 class SolveStats(C.Structure):
@@ -57,7 +57,7 @@ SIGNATURES = {
     "sod_gpu_device_bytes": (C.c_size_t, [VP]),
     "sod_gpu_full_convec_ijk": (C.c_int, [VP] + [VP] * 8 + [C.c_int, C.c_float]),
     "sod_gpu_full_proj_ijk": (C.c_int, [VP] + [VP] * 8),
-    "sod_gpu_full_diff_stab_ijk": (C.c_int, [VP, C.c_float, C.c_float] + [VP] * 15 + [C.c_int, C.c_float]),
+    "sod_gpu_full_diff_stab_ijk": (C.c_int, [VP, C.c_float, C.c_float] + [VP] * 16 + [C.c_int, C.c_float]),
     "sod_gpu_lumped_solver": (C.c_int, [VP, VP, C.c_int]),
     "sod_gpu_updateF": (C.c_int, [VP, VP, VP, VP, VP, C.c_float] + [VP] * 8),
     "sod_gpu_comp_tau": (C.c_int, [VP, VP, VP, VP]),

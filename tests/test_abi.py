@@ -32,3 +32,15 @@ def test_library_exports_header_symbols(header, lib):
 def test_python_binding_declares_every_gpu_symbol():
     from sod2d_b200 import gpu
     assert sorted(gpu.SIGNATURES) == declared("sod2d_gpu.h")
+
+
+def test_binding_argument_counts_match_header():
+    """Each ctypes signature has as many arguments as the C declaration."""
+    from sod2d_b200 import gpu
+    text = (ROOT / "include" / "sod2d_gpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    for name, (_, args) in gpu.SIGNATURES.items():
+        m = re.search(r"\b" + name + r"\s*\(([^)]*)\)", text)
+        assert m, name
+        params = [p for p in m.group(1).split(",") if p.strip() and p.strip() != "void"]
+        assert len(params) == len(args), (name, len(params), len(args))

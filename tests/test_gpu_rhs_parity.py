@@ -110,3 +110,47 @@ def test_comp_tau_matches_oracle(gpu):
     ctx.call("sod_gpu_comp_tau", gpu.dptr(dc), gpu.dptr(du), gpu.dptr(out))
     assert rel_l2(out.cpu().numpy(), ref) < 1e-6
     ctx.close()
+
+
+def test_op_level_entry_points_compose_to_updateF(gpu):
+    """full_convec_ijk + full_proj_ijk + full_diff_stab_ijk + lumped_solver,
+    called as updateF calls them (time_integ_ls.f90:605-686), equal the
+    oracle's updateF."""
+    m, ic, rho, q, E, u, pr, csound = make_case(3, 4, seed=9)
+    om = O.OracleMesh(m)
+    N = m.npoin
+    mu_e = np.random.default_rng(2).uniform(0.0, 2e-3, m.nelem * m.nnode).astype(np.float32)
+    tau = O.comp_tau(om, csound, u)
+    Rm, Rq, Re, proj = O.rhs(om, O.comp_params(ic), rho, q, E, mu_e, ic.mu_factor, tau, want_proj=True)
+    ctx = gpu.Context(m, gpu.phys_from_ic(ic))
+    d = {k: dev(v) for k, v in dict(rho=rho, q=q, E=E, mu_e=mu_e, tau=tau).items()}
+    prim = dict(u=zeros(3 * N), pr=zeros(N), Tem=zeros(N), mu=zeros(N))
+    tmp = dict(Rm=zeros(N), Rq=zeros(3 * N), Re=zeros(N))
+    # primitive fields from the library's EOS (updateF's optional outputs)
+    ctx.call("sod_gpu_updateF", gpu.dptr(d["rho"]), gpu.dptr(d["q"]), gpu.dptr(d["E"]), gpu.dptr(d["mu_e"]),
+             float(ic.mu_factor), gpu.dptr(d["tau"]), gpu.dptr(tmp["Rm"]), gpu.dptr(tmp["Rq"]), gpu.dptr(tmp["Re"]),
+             gpu.dptr(prim["u"]), gpu.dptr(prim["pr"]), gpu.dptr(prim["Tem"]), gpu.dptr(prim["mu"]))
+    h = (prim["pr"] * float(ic.gamma / (ic.gamma - 1.0)) / d["rho"]).contiguous()
+    P5 = [zeros(3 * N) for _ in range(5)]  # ProjMass, ProjEner, ProjMX, ProjMY, ProjMZ
+    ctx.call("sod_gpu_full_proj_ijk", gpu.dptr(d["rho"]), gpu.dptr(prim["u"]), gpu.dptr(prim["Tem"]),
+             *(gpu.dptr(x) for x in P5))
+    w = m.lpoin_w - 1
+    refP = proj.reshape(5, 3, N)
+    for k in range(5):
+        err = rel_l2(P5[k].cpu().numpy().reshape(3, N)[:, w], refP[k][:, w])
+        print("proj", k, err)
+        assert err < TOL
+    R = dict(Rm=zeros(N), Rq=zeros(3 * N), Re=zeros(N))
+    ctx.call("sod_gpu_full_convec_ijk", gpu.dptr(prim["u"]), gpu.dptr(d["q"]), gpu.dptr(d["rho"]),
+             gpu.dptr(prim["pr"]), gpu.dptr(h), gpu.dptr(R["Rm"]), gpu.dptr(R["Rq"]), gpu.dptr(R["Re"]), 1, -1.0)
+    ctx.call("sod_gpu_full_diff_stab_ijk", float(ic.Cp), float(ic.Prt), gpu.dptr(d["rho"]), gpu.dptr(d["rho"]),
+             gpu.dptr(prim["u"]), gpu.dptr(prim["Tem"]), gpu.dptr(prim["mu"]), gpu.dptr(d["mu_e"]), None,
+             *(gpu.dptr(x) for x in P5), gpu.dptr(d["tau"]), gpu.dptr(R["Rm"]), gpu.dptr(R["Rq"]),
+             gpu.dptr(R["Re"]), 0, -1.0)
+    for k, nc in (("Rm", 1), ("Re", 1), ("Rq", 3)):
+        ctx.call("sod_gpu_lumped_solver", gpu.dptr(R[k]), nc)
+    for name, a, b in (("mass", R["Rm"], Rm), ("mom", R["Rq"], Rq), ("ener", R["Re"], Re)):
+        err = rel_l2(a.cpu().numpy(), b)
+        print(f"composed {name}: rel L2 = {err:.3e}")
+        assert err < TOL, (name, err)
+    ctx.close()
