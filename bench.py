@@ -170,7 +170,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def pressure_leg(nelem1d=32, harvest_steps=30, compare_steps=10, dt=0.01, train_steps=300):
+def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_steps=600):
     """Pressure-Poisson solve to a 1e-8 FP64-certified relative residual on
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG against the learned
@@ -191,7 +191,7 @@ def pressure_leg(nelem1d=32, harvest_steps=30, compare_steps=10, dt=0.01, train_
     ctxs = [gpu.Context(m, gpu.default_phys()) for _ in range(2)]
     for c in ctxs:
         c.call("sod_gpu_incomp_init", gpu.dptr(u0), nu)
-    ctxs[0].call("sod_gpu_precond_init", 2024, 64)
+    ctxs[0].call("sod_gpu_precond_init", 2024, 256)
     st = gpu.SolveStats()
     for k in range(harvest_steps):
         for i, c in enumerate(ctxs):
@@ -199,7 +199,7 @@ def pressure_leg(nelem1d=32, harvest_steps=30, compare_steps=10, dt=0.01, train_
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
     loss = C.c_float()
     t0 = time.perf_counter()
-    ctxs[0].call("sod_gpu_precond_train", train_steps, 8, 2e-3, 7, C.byref(loss))
+    ctxs[0].call("sod_gpu_precond_train", train_steps, 16, 3e-3, 7, C.byref(loss))
     train_s = time.perf_counter() - t0
     res = {}
     for i, (name, kind) in enumerate((("jacobi", 0), ("learned", 1))):

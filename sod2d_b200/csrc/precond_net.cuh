@@ -1,189 +1,390 @@
 // Learned element-patch preconditioner for the pressure Poisson problem:
-// forward (inference and training), backward and Adam kernels.
+// inference, training forward/backward and Adam kernels.
 //
-// Network, per element e (P = element order, N = (P+1)^3 nodes):
-//   input  x  = [ (r * Minv)(nodes of e) (N values, tensor order),
-//                 mean of (r * Minv) over each of the 6 face neighbours ]
-//   scale  s  = RMS(x) (the map is positively homogeneous: M(a r) = a M(r))
-//   h1 = tanh(W1 x/s + b1)   (32)
-//   h2 = tanh(W2 h1 + b2)    (32)
-//   y  = W3 h2 + b3          (N)
-//   contribution to z at node(e,a): s * w(e,a) * (x[a]/s + y[a]), w =
-//   1/(elements sharing the node), summed over elements in a fixed order.
-//   The skip term makes the map Jacobi (z = r/diag) when W3 = b3 = 0, the
-//   initial state; training adds a learned correction.
+// For element order P (n1 = P+1, N = n1^3 own nodes) the patch of element e
+// is its N own nodes plus the first node layer of each of its 6 face
+// neighbours, NP = N + 6 n1^2 slots (160 for P=3, 275 for P=4), listed in
+// a per-element patch table (-1 where a face has no neighbour).  With
+// D = Jacobi diagonal, u = D^-1/2 r:
+//   x_e = u on the patch,  h_e = B x_e  (K = 32 modes, B shared, K x NP)
+//   s_e = softplus(MLP(f_e))  (K gains from 8 element geometry features,
+//                              MLP 8 -> 32 -> 32 -> K with tanh)
+//   z   = D^-1/2 ( exp(alpha) u + sum_e P_e^T B^T diag(s_e) B P_e u )
+// M is linear in r and symmetric positive definite for every parameter
+// value; B = 0, alpha = 0 is Jacobi.
 // Parameter vector (FP32), contiguous in this order:
-//   W1T[NIN][H] b1[H] W2T[H][H] b2[H] W3T[H][N] b3[N]
-// (the transposed blocks make the per-lane reads of the forward pass
-// conflict-free in shared memory).
+//   B[K][NP] alpha W1T[F][H] b1[H] W2T[H][H] b2[H] W3T[H][K] b3[K]
 #pragma once
 #include "rhs_kernels.cuh"
 
 namespace sod {
 
-constexpr int NET_H = 32;
+constexpr int NET_H = 32, NET_K = 32, NET_F = 8;
 
 template <int P>
 struct NetDims {
-  static constexpr int N = (P + 1) * (P + 1) * (P + 1);
-  static constexpr int NIN = N + 6;
-  static constexpr int O_W1T = 0;
-  static constexpr int O_B1 = O_W1T + NIN * NET_H;
-  static constexpr int O_W2T = O_B1 + NET_H;
-  static constexpr int O_B2 = O_W2T + NET_H * NET_H;
-  static constexpr int O_W3T = O_B2 + NET_H;
-  static constexpr int O_B3 = O_W3T + NET_H * N;
-  static constexpr int NPARAM = O_B3 + N;
-  // saved activations per element: s, x/s (NIN), h1 (H), h2 (H)
-  static constexpr int NACT = 1 + NIN + 2 * NET_H;
+  static constexpr int N1 = P + 1, N = N1 * N1 * N1, FACE = N1 * N1, NP = N + 6 * FACE;
+  static constexpr int NPP = (NP + 3) / 4 * 4;  // padded patch length for float4 staging
+  static constexpr int O_B = 0, O_ALPHA = NET_K * NP, O_W1T = O_ALPHA + 1, O_B1 = O_W1T + NET_F * NET_H,
+                       O_W2T = O_B1 + NET_H, O_B2 = O_W2T + NET_H * NET_H, O_W3T = O_B2 + NET_H,
+                       O_B3 = O_W3T + NET_H * NET_K, NPARAM = O_B3 + NET_K;
+  static constexpr int NMLP = NPARAM - O_W1T;
+  static constexpr int EPW = 4;  // elements per warp in the patch kernels
+  // dynamic shared memory of the patch kernels (bytes) for `warps` warps
+  static constexpr size_t apply_smem(int warps) {
+    return (size_t)(2 * NPP * NET_K + warps * EPW * (NPP + NET_K)) * 4;
+  }
+  static constexpr size_t bwd_smem(int warps) { return (size_t)(NPP * NET_K + warps * EPW * 2 * NPP) * 4; }
 };
 
-// Mean of (r*Minv) over each element.
-__global__ void k_elem_mean(MeshDev m, int N, const double *__restrict__ r, const double *__restrict__ Minv,
-                            float *__restrict__ mean) {
+__device__ __forceinline__ float softplusf(float a) { return a > 20.f ? a : log1pf(expf(a)); }
+__device__ __forceinline__ float sigmoidf(float a) { return 1.f / (1.f + expf(-a)); }
+
+// Raw geometry features per element (FP64), warp per element: mean
+// reference metric G_jk = sum_i dxi_j/dx_i dxi_k/dx_i over the Gauss points,
+// vol = sum gpvol.  raw = [log(3 G_bb / tr G) (3), G_01, G_02, G_12
+// correlations, log vol, log(tr G) + 2/3 log vol].
+template <int P>
+__global__ void k_elem_features(MeshDev m, double *__restrict__ raw) {
+  constexpr int N = Cfg<P>::N;
   const long long e = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
   if (e >= m.nelem) return;
-  float s = 0.f;
+  double g[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int t = lane; t < N; t += 32) {
-    const int p = m.conn[e * N + t];
-    s += (float)(r[p] * Minv[p]);
+    const float *q = m.geo + e * 10 * N + t;
+    double h[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) h[c] = (double)q[c * N];
+    auto G = [&](int j, int k) { return h[3 * j] * h[3 * k] + h[3 * j + 1] * h[3 * k + 1] + h[3 * j + 2] * h[3 * k + 2]; };
+    g[0] += G(0, 0); g[1] += G(1, 1); g[2] += G(2, 2);
+    g[3] += G(0, 1); g[4] += G(0, 2); g[5] += G(1, 2);
+    g[6] += (double)q[9 * N];
   }
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) mean[e] = s / (float)N;
+#pragma unroll
+  for (int c = 0; c < 7; ++c)
+    for (int o = 16; o > 0; o >>= 1) g[c] += __shfl_xor_sync(0xffffffffu, g[c], o);
+  if (lane == 0) {
+    for (int c = 0; c < 6; ++c) g[c] /= (double)N;
+    const double tr = g[0] + g[1] + g[2];
+    double *o = raw + e * NET_F;
+    o[0] = log(3.0 * g[0] / tr);
+    o[1] = log(3.0 * g[1] / tr);
+    o[2] = log(3.0 * g[2] / tr);
+    o[3] = g[3] / sqrt(g[0] * g[1]);
+    o[4] = g[4] / sqrt(g[0] * g[2]);
+    o[5] = g[5] / sqrt(g[1] * g[2]);
+    o[6] = log(g[6]);
+    o[7] = log(tr) + (2.0 / 3.0) * log(g[6]);
+  }
 }
 
-// Forward pass, one warp per element (grid-stride), parameters staged in
-// shared memory.  TRAIN saves the activations needed by the backward pass.
-template <int P, bool TRAIN>
-__global__ void __launch_bounds__(256)
-k_net_fwd(MeshDev m, const int *__restrict__ nbr, const float *__restrict__ emean, const double *__restrict__ r,
-          const double *__restrict__ Minv, const float *__restrict__ wts, const float *__restrict__ params,
-          float *__restrict__ out_slots, float *__restrict__ act) {
+// Per-element mode gains s_e = softplus(MLP(f_e)), warp per element (lane =
+// hidden unit / mode).
+template <int P>
+__global__ void k_mlp_gains(long long nelem, const float *__restrict__ feat, const float *__restrict__ prm,
+                            float *__restrict__ gains) {
   using D = NetDims<P>;
-  constexpr int N = D::N, NIN = D::NIN, H = NET_H;
-  extern __shared__ float smem[];
-  float *W = smem;                              // NPARAM
-  float *scr = smem + D::NPARAM;                // per warp: NIN + 2H
-  for (int i = threadIdx.x; i < D::NPARAM; i += blockDim.x) W[i] = params[i];
-  __syncthreads();
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarps = blockDim.x / 32;
-  float *x = scr + warp * (NIN + 2 * H), *h1 = x + NIN, *h2 = h1 + H;
-  for (long long e = (long long)blockIdx.x * nwarps + warp; e < m.nelem; e += (long long)gridDim.x * nwarps) {
-    float ss = 0.f;
-    for (int t = lane; t < N; t += 32) {
-      const int p = m.conn[e * N + t];
-      const float v = (float)(r[p] * Minv[p]);
-      x[t] = v;
-      ss += v * v;
-    }
-    if (lane < 6) {
-      const float v = emean[nbr[e * 6 + lane]];
-      x[N + lane] = v;
-      ss += v * v;
-    }
-    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
-    const float s = sqrtf(ss / (float)NIN);
-    const float inv = s > 0.f ? 1.f / s : 0.f;
-    __syncwarp();
-    for (int t = lane; t < NIN; t += 32) x[t] *= inv;
-    __syncwarp();
-    float a = W[D::O_B1 + lane];
-    for (int i = 0; i < NIN; ++i) a = fmaf(W[D::O_W1T + i * H + lane], x[i], a);
-    h1[lane] = tanhf(a);
-    __syncwarp();
-    a = W[D::O_B2 + lane];
+  constexpr int H = NET_H, K = NET_K;
+  const long long e = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (e >= nelem) return;
+  float a = prm[D::O_B1 + lane];
+#pragma unroll
+  for (int f = 0; f < NET_F; ++f) a = fmaf(prm[D::O_W1T + f * H + lane], feat[e * NET_F + f], a);
+  const float h1 = tanhf(a);
+  a = prm[D::O_B2 + lane];
 #pragma unroll 8
-    for (int i = 0; i < H; ++i) a = fmaf(W[D::O_W2T + i * H + lane], h1[i], a);
-    h2[lane] = tanhf(a);
-    __syncwarp();
-    for (int o = lane; o < N; o += 32) {
-      float y = W[D::O_B3 + o];
+  for (int i = 0; i < H; ++i) a = fmaf(prm[D::O_W2T + i * H + lane], __shfl_sync(0xffffffffu, h1, i), a);
+  const float h2 = tanhf(a);
+  a = prm[D::O_B3 + lane];
 #pragma unroll 8
-      for (int j = 0; j < H; ++j) y = fmaf(W[D::O_W3T + j * N + o], h2[j], y);
-      out_slots[e * N + o] = s * wts[e * N + o] * (x[o] + y);
+  for (int i = 0; i < H; ++i) a = fmaf(prm[D::O_W3T + i * K + lane], __shfl_sync(0xffffffffu, h2, i), a);
+  gains[e * K + lane] = softplusf(a);
+}
+
+// Stage B into shared memory: BT[j][k] (encoder, lane = mode) and, when
+// DEC, Bk[k][j] (decoder, lane = patch slot); rows/columns >= NP are zero.
+template <int P, bool DEC>
+__device__ void stage_B(const float *__restrict__ prm, float *BT, float *Bk) {
+  using D = NetDims<P>;
+  for (int i = threadIdx.x; i < D::NPP * NET_K; i += blockDim.x) {
+    const int j = i / NET_K, k = i % NET_K;
+    BT[i] = j < D::NP ? prm[D::O_B + k * D::NP + j] : 0.f;
+  }
+  if (DEC)
+    for (int i = threadIdx.x; i < NET_K * D::NPP; i += blockDim.x) {
+      const int k = i / D::NPP, j = i % D::NPP;
+      Bk[i] = j < D::NP ? prm[D::O_B + k * D::NP + j] : 0.f;
     }
-    if (TRAIN) {
-      float *ac = act + e * D::NACT;
-      if (lane == 0) ac[0] = s;
-      for (int t = lane; t < NIN; t += 32) ac[1 + t] = x[t];
-      ac[1 + NIN + lane] = h1[lane];
-      ac[1 + NIN + H + lane] = h2[lane];
+}
+
+// Gather D^-1/2 v over the patches of EPW elements into xs[EPW][NPP].
+template <int P>
+__device__ __forceinline__ void gather_patch(long long e0, long long nelem, const int *__restrict__ pt,
+                                             const double *__restrict__ v, const double *__restrict__ Dh, float *xs,
+                                             int lane) {
+  using D = NetDims<P>;
+#pragma unroll
+  for (int el = 0; el < D::EPW; ++el) {
+    const long long e = e0 + el;
+    for (int j = lane; j < D::NPP; j += 32) {
+      float x = 0.f;
+      if (e < nelem && j < D::NP) {
+        const int idx = pt[e * D::NP + j];
+        if (idx >= 0) x = (float)(Dh[idx] * v[idx]);
+      }
+      xs[el * D::NPP + j] = x;
     }
-    __syncwarp();
   }
 }
 
-// Backward pass: g = dL/dz at nodes (FP64).  Each warp accumulates the
-// parameter gradient of its elements in its own shared-memory slice; the
-// block sums its slices in warp order and writes one partial per block
-// (deterministic).  Shared memory: params + transposed copies + nwarps
-// gradient slices.
+// h[el] = sum_j B[lane][j] xs[el][j]
+template <int P>
+__device__ __forceinline__ void encode(const float *BT, const float *xs, int lane, float (&h)[NetDims<P>::EPW]) {
+  using D = NetDims<P>;
+#pragma unroll
+  for (int el = 0; el < D::EPW; ++el) h[el] = 0.f;
+#pragma unroll 2
+  for (int j = 0; j < D::NPP; j += 4) {
+    const float b0 = BT[(j + 0) * NET_K + lane], b1 = BT[(j + 1) * NET_K + lane];
+    const float b2 = BT[(j + 2) * NET_K + lane], b3 = BT[(j + 3) * NET_K + lane];
+#pragma unroll
+    for (int el = 0; el < D::EPW; ++el) {
+      const float4 x = *reinterpret_cast<const float4 *>(xs + el * D::NPP + j);
+      h[el] = fmaf(b0, x.x, fmaf(b1, x.y, fmaf(b2, x.z, fmaf(b3, x.w, h[el]))));
+    }
+  }
+}
+
+// Inference: per element o_e = B^T diag(s_e) B x_e written to patch slots
+// [e][NP] (FP32).  EPW elements per warp, grid-stride over element groups.
 template <int P>
 __global__ void __launch_bounds__(256)
-k_net_bwd(MeshDev m, const double *__restrict__ g, const float *__restrict__ wts, const float *__restrict__ params,
-          const float *__restrict__ act, float *__restrict__ part) {
+k_patch_apply(long long nelem, const int *__restrict__ pt, const double *__restrict__ r,
+              const double *__restrict__ Dh, const float *__restrict__ prm, const float *__restrict__ gains,
+              float *__restrict__ slots) {
   using D = NetDims<P>;
-  constexpr int N = D::N, NIN = D::NIN, H = NET_H, NP = D::NPARAM;
-  extern __shared__ float smem[];
+  constexpr int NPP = D::NPP, K = NET_K, EPW = D::EPW;
+  extern __shared__ __align__(16) float smem[];
+  float *BT = smem, *Bk = smem + NPP * K;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarps = blockDim.x / 32;
-  float *W = smem;                 // NP (transposed layout as the parameter vector)
-  float *W3 = W + NP;              // [N][H] row-major (a, j)
-  float *W2 = W3 + N * H;          // [H][H] row-major (j, i)
-  float *G = W2 + H * H;           // nwarps x NP gradient slices
-  float *scr = G + nwarps * NP;    // per warp: N (dy) + 2H
-  for (int i = threadIdx.x; i < NP; i += blockDim.x) W[i] = params[i];
+  float *xs = Bk + K * NPP + warp * EPW * (NPP + K), *ys = xs + EPW * NPP;
+  stage_B<P, true>(prm, BT, Bk);
   __syncthreads();
-  for (int i = threadIdx.x; i < N * H; i += blockDim.x) {
-    const int a = i / H, j = i % H;
-    W3[i] = W[D::O_W3T + j * N + a];
-  }
-  for (int i = threadIdx.x; i < H * H; i += blockDim.x) {
-    const int j = i / H, ii = i % H;
-    W2[i] = W[D::O_W2T + ii * H + j];
-  }
-  for (int i = threadIdx.x; i < nwarps * NP; i += blockDim.x) G[i] = 0.f;
-  __syncthreads();
-  float *Gw = G + warp * NP;
-  float *dy = scr + warp * (N + 2 * H), *dz2 = dy + N, *dz1 = dz2 + H;
-  for (long long e = (long long)blockIdx.x * nwarps + warp; e < m.nelem; e += (long long)gridDim.x * nwarps) {
-    const float *ac = act + e * D::NACT;
-    const float s = ac[0];
-    const float *x = ac + 1, *h1 = x + NIN, *h2 = h1 + H;
-    for (int o = lane; o < N; o += 32) {
-      const int p = m.conn[e * N + o];
-      dy[o] = (float)g[p] * s * wts[e * N + o];
+  for (long long g = (long long)blockIdx.x * nwarps + warp; g * EPW < nelem; g += (long long)gridDim.x * nwarps) {
+    const long long e0 = g * EPW;
+    gather_patch<P>(e0, nelem, pt, r, Dh, xs, lane);
+    __syncwarp();
+    float h[EPW];
+    encode<P>(BT, xs, lane, h);
+#pragma unroll
+    for (int el = 0; el < EPW; ++el) ys[el * K + lane] = (e0 + el < nelem) ? gains[(e0 + el) * K + lane] * h[el] : 0.f;
+    __syncwarp();
+    for (int j = lane; j < D::NP; j += 32) {
+      float o[EPW];
+#pragma unroll
+      for (int el = 0; el < EPW; ++el) o[el] = 0.f;
+#pragma unroll 2
+      for (int k = 0; k < K; k += 4) {
+        const float b0 = Bk[(k + 0) * NPP + j], b1 = Bk[(k + 1) * NPP + j];
+        const float b2 = Bk[(k + 2) * NPP + j], b3 = Bk[(k + 3) * NPP + j];
+#pragma unroll
+        for (int el = 0; el < EPW; ++el) {
+          const float4 y = *reinterpret_cast<const float4 *>(ys + el * K + k);
+          o[el] = fmaf(b0, y.x, fmaf(b1, y.y, fmaf(b2, y.z, fmaf(b3, y.w, o[el]))));
+        }
+      }
+#pragma unroll
+      for (int el = 0; el < EPW; ++el)
+        if (e0 + el < nelem) slots[(e0 + el) * D::NP + j] = o[el];
     }
     __syncwarp();
-    // layer 3: dW3T[j][a] += dy[a] h2[j], db3[a] += dy[a]
-    for (int o = lane; o < N; o += 32) {
-      Gw[D::O_B3 + o] += dy[o];
-      for (int j = 0; j < H; ++j) Gw[D::O_W3T + j * N + o] += dy[o] * h2[j];
-    }
-    float dh2 = 0.f;
-    for (int o = 0; o < N; ++o) dh2 = fmaf(W3[o * H + lane], dy[o], dh2);
-    const float hv2 = h2[lane];
-    dz2[lane] = dh2 * (1.f - hv2 * hv2);
+  }
+}
+
+// z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of the node's patch
+// slots), FP64, for nodes that own patch slots (the working nodes).
+__global__ void k_patch_gather(long long npoin, const int *__restrict__ pptr, const int *__restrict__ pslot,
+                               const float *__restrict__ slots, const double *__restrict__ r,
+                               const double *__restrict__ Dh, const float *__restrict__ prm, int o_alpha,
+                               double *__restrict__ z) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= npoin) return;
+  const int b = pptr[n], en = pptr[n + 1];
+  if (b == en) return;
+  double acc = 0.0;
+  for (int s = b; s < en; ++s) acc += (double)slots[pslot[s]];
+  const double d = Dh[n];
+  z[n] = d * (exp((double)prm[o_alpha]) * d * r[n] + acc);
+}
+
+// Training, per element: x = patch of D^-1/2 r, w = patch of D^-1/2 g
+// (g = dL/dz), h = B x, a = B w; stores X, W (patch rows), Y = s h,
+// SA = s a and dS = h a (dL/ds).
+template <int P>
+__global__ void __launch_bounds__(256)
+k_patch_bwd_elem(long long nelem, const int *__restrict__ pt, const double *__restrict__ r,
+                 const double *__restrict__ g, const double *__restrict__ Dh, const float *__restrict__ prm,
+                 const float *__restrict__ gains, float *__restrict__ X, float *__restrict__ W,
+                 float *__restrict__ Y, float *__restrict__ SA, float *__restrict__ dS) {
+  using D = NetDims<P>;
+  constexpr int NPP = D::NPP, K = NET_K, EPW = D::EPW;
+  extern __shared__ __align__(16) float smem[];
+  float *BT = smem;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarps = blockDim.x / 32;
+  float *xs = BT + NPP * K + warp * EPW * 2 * NPP, *ws = xs + EPW * NPP;
+  stage_B<P, false>(prm, BT, nullptr);
+  __syncthreads();
+  for (long long gi = (long long)blockIdx.x * nwarps + warp; gi * EPW < nelem; gi += (long long)gridDim.x * nwarps) {
+    const long long e0 = gi * EPW;
+    gather_patch<P>(e0, nelem, pt, r, Dh, xs, lane);
+    gather_patch<P>(e0, nelem, pt, g, Dh, ws, lane);
     __syncwarp();
-    // layer 2: dW2T[i][j] += dz2[j] h1[i]
-    Gw[D::O_B2 + lane] += dz2[lane];
-    for (int i = 0; i < H; ++i) Gw[D::O_W2T + i * H + lane] += dz2[lane] * h1[i];
+    float h[EPW], a[EPW];
+    encode<P>(BT, xs, lane, h);
+    encode<P>(BT, ws, lane, a);
+#pragma unroll
+    for (int el = 0; el < EPW; ++el) {
+      const long long e = e0 + el;
+      if (e >= nelem) continue;
+      const float s = gains[e * K + lane];
+      Y[e * K + lane] = s * h[el];
+      SA[e * K + lane] = s * a[el];
+      dS[e * K + lane] = h[el] * a[el];
+      for (int j = lane; j < D::NP; j += 32) {
+        X[e * D::NP + j] = xs[el * NPP + j];
+        W[e * D::NP + j] = ws[el * NPP + j];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// dB[k][j] = sum_e Y[e][k] W[e][j] + SA[e][k] X[e][j]; block b sums the
+// contiguous element range [b E / nb, (b+1) E / nb) in element order and
+// writes its partial to part[b * stride + O_B + k NP + j] (deterministic).
+template <int P>
+__global__ void __launch_bounds__(256)
+k_patch_dB(long long nelem, const float *__restrict__ X, const float *__restrict__ W, const float *__restrict__ Y,
+           const float *__restrict__ SA, float *__restrict__ part, long long stride) {
+  using D = NetDims<P>;
+  constexpr int NP = D::NP, K = NET_K, CH = 8, ENT = (K * NP + 255) / 256;
+  __shared__ __align__(16) float Xs[CH][NP], Ws[CH][NP], Ys[CH][K], Ss[CH][K];
+  const long long lo = nelem * blockIdx.x / gridDim.x, hi = nelem * (blockIdx.x + 1) / gridDim.x;
+  float acc[ENT];
+#pragma unroll
+  for (int q = 0; q < ENT; ++q) acc[q] = 0.f;
+  for (long long c0 = lo; c0 < hi; c0 += CH) {
+    const int nc = (int)((hi - c0) < CH ? (hi - c0) : CH);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nc * NP; i += blockDim.x) {
+      const int el = i / NP, j = i % NP;
+      Xs[el][j] = X[(c0 + el) * NP + j];
+      Ws[el][j] = W[(c0 + el) * NP + j];
+    }
+    for (int i = threadIdx.x; i < nc * K; i += blockDim.x) {
+      const int el = i / K, k = i % K;
+      Ys[el][k] = Y[(c0 + el) * K + k];
+      Ss[el][k] = SA[(c0 + el) * K + k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < ENT; ++q) {
+      const int idx = threadIdx.x + 256 * q;
+      if (idx < K * NP) {
+        const int k = idx / NP, j = idx % NP;
+        float s = acc[q];
+        for (int el = 0; el < nc; ++el) s = fmaf(Ys[el][k], Ws[el][j], fmaf(Ss[el][k], Xs[el][j], s));
+        acc[q] = s;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < ENT; ++q) {
+    const int idx = threadIdx.x + 256 * q;
+    if (idx < K * NP) part[blockIdx.x * stride + D::O_B + idx] = acc[q];
+  }
+}
+
+// Gradient of the gain MLP from dS = dL/ds; block b covers the same element
+// range as k_patch_dB, each warp accumulates its elements in a shared-memory
+// slice, the block sums the slices in warp order into part (deterministic).
+template <int P>
+__global__ void __launch_bounds__(256)
+k_mlp_bwd(long long nelem, const float *__restrict__ feat, const float *__restrict__ prm,
+          const float *__restrict__ dS, float *__restrict__ part, long long stride) {
+  using D = NetDims<P>;
+  constexpr int H = NET_H, K = NET_K, NM = D::NMLP;
+  constexpr int R_W1T = 0, R_B1 = R_W1T + NET_F * H, R_W2T = R_B1 + H, R_B2 = R_W2T + H * H, R_W3T = R_B2 + H,
+                R_B3 = R_W3T + H * K;
+  extern __shared__ __align__(16) float smem[];
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarps = blockDim.x / 32;
+  float *Gw = smem + warp * NM;
+  for (int i = threadIdx.x; i < nwarps * NM; i += blockDim.x) smem[i] = 0.f;
+  __syncthreads();
+  const long long lo = nelem * blockIdx.x / gridDim.x, hi = nelem * (blockIdx.x + 1) / gridDim.x;
+  const float *W2T = prm + D::O_W2T, *W3T = prm + D::O_W3T;
+  for (long long e = lo + warp; e < hi; e += nwarps) {
+    float f[NET_F];
+#pragma unroll
+    for (int q = 0; q < NET_F; ++q) f[q] = feat[e * NET_F + q];
+    float a = prm[D::O_B1 + lane];
+#pragma unroll
+    for (int q = 0; q < NET_F; ++q) a = fmaf(prm[D::O_W1T + q * H + lane], f[q], a);
+    const float h1 = tanhf(a);
+    a = prm[D::O_B2 + lane];
+    for (int i = 0; i < H; ++i) a = fmaf(W2T[i * H + lane], __shfl_sync(0xffffffffu, h1, i), a);
+    const float h2 = tanhf(a);
+    a = prm[D::O_B3 + lane];
+    for (int i = 0; i < H; ++i) a = fmaf(W3T[i * K + lane], __shfl_sync(0xffffffffu, h2, i), a);
+    const float dO = dS[e * K + lane] * sigmoidf(a);  // lane = mode
+    // layer 3
+    Gw[R_B3 + lane] += dO;
+    for (int i = 0; i < H; ++i) Gw[R_W3T + i * K + lane] += __shfl_sync(0xffffffffu, h2, i) * dO;
+    float dh2 = 0.f;  // lane = hidden unit i
+    for (int k = 0; k < K; ++k) dh2 = fmaf(W3T[lane * K + k], __shfl_sync(0xffffffffu, dO, k), dh2);
+    const float dz2 = dh2 * (1.f - h2 * h2);
+    // layer 2
+    Gw[R_B2 + lane] += dz2;
+    for (int i = 0; i < H; ++i) Gw[R_W2T + i * H + lane] += __shfl_sync(0xffffffffu, h1, i) * dz2;
     float dh1 = 0.f;
-    for (int j = 0; j < H; ++j) dh1 = fmaf(W2[j * H + lane], dz2[j], dh1);
-    const float hv1 = h1[lane];
-    dz1[lane] = dh1 * (1.f - hv1 * hv1);
-    __syncwarp();
-    // layer 1: dW1T[i][j] += dz1[j] x[i]
-    Gw[D::O_B1 + lane] += dz1[lane];
-    for (int i = 0; i < NIN; ++i) Gw[D::O_W1T + i * H + lane] += dz1[lane] * x[i];
+    for (int j = 0; j < H; ++j) dh1 = fmaf(W2T[lane * H + j], __shfl_sync(0xffffffffu, dz2, j), dh1);
+    const float dz1 = dh1 * (1.f - h1 * h1);
+    // layer 1
+    Gw[R_B1 + lane] += dz1;
+#pragma unroll
+    for (int q = 0; q < NET_F; ++q) Gw[R_W1T + q * H + lane] += f[q] * dz1;
     __syncwarp();
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+  for (int i = threadIdx.x; i < NM; i += blockDim.x) {
     float s = 0.f;
-    for (int w = 0; w < nwarps; ++w) s += G[w * NP + i];
-    part[(long long)blockIdx.x * NP + i] = s;
+    for (int w = 0; w < nwarps; ++w) s += smem[w * NM + i];
+    part[blockIdx.x * stride + D::O_W1T + i] = s;
   }
+}
+
+// dL/dalpha partial: exp(alpha) sum over the block's working nodes of
+// (D^-1/2 g)(D^-1/2 r), written to part[b * stride + o_alpha].
+__global__ void k_alpha_part(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
+                             const double *__restrict__ g, const double *__restrict__ Dh,
+                             const float *__restrict__ prm, int o_alpha, float *__restrict__ part, long long stride) {
+  __shared__ double sh[256];
+  const long long lo = (long long)npoin_w * blockIdx.x / gridDim.x,
+                  hi = (long long)npoin_w * (blockIdx.x + 1) / gridDim.x;
+  double s = 0.0;
+  for (long long t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+    const int n = lpoin_w[t];
+    s += (Dh[n] * g[n]) * (Dh[n] * r[n]);
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x * stride + o_alpha] = (float)(exp((double)prm[o_alpha]) * sh[0]);
 }
 
 // grad[i] = sum over blocks of part[b][i] (fixed order), then Adam.

@@ -74,19 +74,21 @@ struct sod_gpu_ctx {
   } cg;
   // learned preconditioner
   struct Net {
-    bool ready = false;
-    int nparam = 0, nblk_bwd = 0, bwd_threads = 256, step = 0;
-    float *params = nullptr, *m1 = nullptr, *m2 = nullptr, *part = nullptr, *wts = nullptr, *emean = nullptr,
-          *act = nullptr, *grad = nullptr;
-    int *nbr = nullptr;
-    // harvest ring of (r, e) pairs, FP32, and e^T A e per pair
-    int cap = 0, count = 0, next = 0;
+    bool ready = false, gains_ok = false;
+    int nparam = 0, nblk_bwd = 148, step = 0, NP = 0;
+    float *params = nullptr, *m1 = nullptr, *m2 = nullptr, *part = nullptr, *grad = nullptr;
+    int *pt = nullptr, *pptr = nullptr, *pslot = nullptr;   // patch table [E][NP]; node -> patch-slot CSR
+    float *feat = nullptr, *gains = nullptr;                  // [E][8], [E][32]
+    float *X = nullptr, *W = nullptr, *Y = nullptr, *SA = nullptr, *dS = nullptr;  // training scratch
+    double *Dh = nullptr;                                     // D^-1/2
+    // harvested (r, e) pairs, FP32, reservoir-sampled, and e^T A e per pair
+    int cap = 0, count = 0;
+    long long offered = 0;
+    uint64_t rs_state = 0x9e3779b97f4a7c15ULL;
     float *hr = nullptr, *he = nullptr;
     std::vector<double> eAe;
     double *xsnap = nullptr;  // solver snapshots (FP64) while harvesting
     double *tmp1 = nullptr, *tmp2 = nullptr;
-    float *zf = nullptr;
-    int harvest_every_solve = 0;
   } net;
   // incompressible projection-step state
   struct Inc {
@@ -800,14 +802,6 @@ __global__ void k_ones_dot(int npoin_w, const int *__restrict__ lpoin_w, const d
   if (threadIdx.x == 0) part[0] = sh[0];
 }
 
-__global__ void k_copy_cast_w(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ a,
-                              double *__restrict__ b) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npoin_w) return;
-  const int i = lpoin_w[t];
-  b[i] = (double)a[i];
-}
-
 __global__ void k_jacobi64(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ Minv,
                            const double *__restrict__ r, double *__restrict__ z) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -881,9 +875,17 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
   auto take_snapshot = [&](int iter_no) {
     if (!harvest || (int)snaps.size() >= 16 || iter_no != next_snap) return;
     next_snap = next_snap < 8 ? next_snap + 1 : next_snap * 2;
-    const int slot = NT.next;
-    NT.next = (NT.next + 1) % NT.cap;
-    if (NT.count < NT.cap) NT.count++;
+    // reservoir sampling over every pair offered so far (seeded, reproducible)
+    int slot;
+    if (NT.count < NT.cap) {
+      slot = NT.count++;
+    } else {
+      NT.rs_state = NT.rs_state * 6364136223846793005ULL + 1442695040888963407ULL;
+      const long long j = (long long)((NT.rs_state >> 11) % (uint64_t)(NT.offered + 1));
+      slot = j < NT.cap ? (int)j : -1;
+    }
+    NT.offered++;
+    if (slot < 0) return;
     const int si = (int)snaps.size();
     k_d2f_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.r, NT.hr + (size_t)slot * N);
     cudaMemcpyAsync(NT.xsnap + (size_t)si * N, x, N * 8, cudaMemcpyDeviceToDevice, st);
@@ -1059,6 +1061,8 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
 
 namespace {
 
+int ensure_gains(sod_gpu_ctx *c);
+
 int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z) {
   if (kind == 0) {
     k_jacobi64<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, c->cg.Minv, r, z);
@@ -1066,18 +1070,18 @@ int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z) {
   }
   auto &NT = c->net;
   if (!NT.ready) return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
-  k_elem_mean<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), c->N, r, c->cg.Minv, NT.emean);
+  int rc;
+  if ((rc = ensure_gains(c))) return rc;
   dispatch(c, [&](auto L) {
     using LL = decltype(L);
     constexpr int P = LL::P_;
     using D = NetDims<P>;
-    const size_t sm = (size_t)(D::NPARAM + 8 * (D::NIN + 2 * NET_H)) * 4;
-    k_net_fwd<P, false><<<592, 256, sm, c->stream>>>(c->md(), NT.nbr, NT.emean, r, c->cg.Minv, NT.wts, NT.params,
-                                                     c->slotsB, nullptr);
+    k_patch_apply<P><<<4 * 148, 256, D::apply_smem(8), c->stream>>>(c->nelem, NT.pt, r, NT.Dh, NT.params, NT.gains,
+                                                                    c->slotsB);
+    k_patch_gather<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, NT.pptr, NT.pslot, c->slotsB, r, NT.Dh,
+                                                               NT.params, D::O_ALPHA, z);
     return 0;
   });
-  k_gather1<float><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, NT.zf, 0);
-  k_copy_cast_w<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, NT.zf, z);
   return 0;
 }
 
@@ -1389,41 +1393,6 @@ int sod_gpu_comp_get_state(sod_gpu_ctx *c, float *rho, float *q, float *E, float
 
 namespace {
 
-template <int P>
-size_t bwd_smem(int nwarps) {
-  using D = NetDims<P>;
-  return (size_t)(D::NPARAM + D::N * NET_H + NET_H * NET_H + nwarps * D::NPARAM + nwarps * (D::N + 2 * NET_H)) * 4;
-}
-
-// Forward (training), z = assembled output at working nodes (FP64).
-void net_forward_train(sod_gpu_ctx *c, const double *r, double *z) {
-  auto &NT = c->net;
-  k_elem_mean<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), c->N, r, c->cg.Minv, NT.emean);
-  dispatch(c, [&](auto L) {
-    using LL = decltype(L);
-    constexpr int P = LL::P_;
-    using D = NetDims<P>;
-    const size_t sm = (size_t)(D::NPARAM + 8 * (D::NIN + 2 * NET_H)) * 4;
-    k_net_fwd<P, true><<<592, 256, sm, c->stream>>>(c->md(), NT.nbr, NT.emean, r, c->cg.Minv, NT.wts, NT.params,
-                                                    c->slotsB, NT.act);
-    return 0;
-  });
-  k_gather1<float><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, NT.zf, 0);
-  k_copy_cast_w<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, NT.zf, z);
-}
-
-void net_backward(sod_gpu_ctx *c, const double *g, float *part) {
-  auto &NT = c->net;
-  dispatch(c, [&](auto L) {
-    using LL = decltype(L);
-    constexpr int P = LL::P_;
-    const int nw = NT.bwd_threads / 32;
-    k_net_bwd<P><<<NT.nblk_bwd, NT.bwd_threads, bwd_smem<P>(nw), c->stream>>>(c->md(), g, NT.wts, NT.params,
-                                                                             NT.act, part);
-    return 0;
-  });
-}
-
 __global__ void k_loss_grad_vec(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ Ad,
                                 double scale, double *__restrict__ g) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1448,24 +1417,158 @@ __global__ void k_d2f_w(int npoin_w, const int *__restrict__ lpoin_w, const doub
   b[i] = (float)a[i];
 }
 
-// loss = d^T A d / eAe with d = e - z; writes g = dL/dz = -2 A d / eAe into
-// NT.tmp2, and the per-block parameter-gradient partials into part.
+__global__ void k_inv_sqrt_diag(long long n, const float *__restrict__ diag, double *__restrict__ Dh) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) Dh[i] = diag[i] > 0.f ? 1.0 / sqrt((double)diag[i]) : 0.0;
+}
+
+int ensure_gains(sod_gpu_ctx *c) {
+  auto &NT = c->net;
+  if (NT.gains_ok) return 0;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_mlp_gains<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->nelem, NT.feat, NT.params, NT.gains);
+    return 0;
+  });
+  NT.gains_ok = true;
+  return 0;
+}
+
+int ensure_train_scratch(sod_gpu_ctx *c) {
+  auto &NT = c->net;
+  if (NT.X) return 0;
+  const size_t E = (size_t)c->nelem;
+  int rc;
+  if ((rc = c->alloc(&NT.X, E * NT.NP)) || (rc = c->alloc(&NT.W, E * NT.NP)) || (rc = c->alloc(&NT.Y, E * NET_K)) ||
+      (rc = c->alloc(&NT.SA, E * NET_K)) || (rc = c->alloc(&NT.dS, E * NET_K)))
+    return rc;
+  return 0;
+}
+
+// Parameter-gradient partials of g = dL/dz at the residual r into part
+// (nblk_bwd rows of nparam floats).
+void net_backward(sod_gpu_ctx *c, const double *r, const double *g, float *part) {
+  auto &NT = c->net;
+  const long long stride = NT.nparam;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    constexpr int P = LL::P_;
+    using D = NetDims<P>;
+    k_patch_bwd_elem<P><<<4 * 148, 256, D::bwd_smem(8), c->stream>>>(c->nelem, NT.pt, r, g, NT.Dh, NT.params,
+                                                                     NT.gains, NT.X, NT.W, NT.Y, NT.SA, NT.dS);
+    k_patch_dB<P><<<NT.nblk_bwd, 256, 0, c->stream>>>(c->nelem, NT.X, NT.W, NT.Y, NT.SA, part, stride);
+    k_mlp_bwd<P><<<NT.nblk_bwd, 256, (size_t)8 * D::NMLP * 4, c->stream>>>(c->nelem, NT.feat, NT.params, NT.dS,
+                                                                           part, stride);
+    k_alpha_part<<<NT.nblk_bwd, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, r, g, NT.Dh, NT.params, D::O_ALPHA,
+                                                     part, stride);
+    return 0;
+  });
+}
+
+// loss = d^T A d / eAe with d = e - M r; the gradient partials go to part.
 int net_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double eAe, float *part, double *loss) {
   auto &NT = c->net;
   auto &G = c->cg;
   const int nw = c->npoin_w;
   const unsigned nb = nblk(nw, 256);
-  net_forward_train(c, r, NT.tmp1);                                            // z
-  k_axpby<double><<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, 1.0, e, -1.0, NT.tmp1);  // d = e - z
-  lap<double>(c, NT.tmp1, NT.tmp2);                                            // A d
+  int rc;
+  if ((rc = ensure_train_scratch(c)) || (rc = apply_precond(c, 1, r, NT.tmp1))) return rc;  // z
+  k_axpby<double><<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, 1.0, e, -1.0, NT.tmp1);        // d = e - z
+  lap<double>(c, NT.tmp1, NT.tmp2);                                                         // A d
   dots<double, 1>(c, DotArgs<double, 1>{{NT.tmp1}, {NT.tmp2}, {nullptr}}, G.dots + 2);
   k_loss_grad_vec<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, NT.tmp2, -2.0 / eAe, NT.tmp2);
-  net_backward(c, NT.tmp2, part);
+  net_backward(c, r, NT.tmp2, part);
   if (loss) {
     double h;
     CUDA_TRY(cudaMemcpyAsync(&h, G.dots + 2, 8, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     *loss = h / eAe;
+  }
+  return 0;
+}
+
+// Face neighbours (element itself on a boundary) and the patch table: own
+// nodes in tensor order, then for each face f the first node layer of the
+// neighbour across f, at the face's tangential coordinates (a, b) of this
+// element's frame (-1 without a neighbour).  The neighbour's layer is found
+// from the affine map between the two elements' face corners, so any
+// relative orientation of conforming hexahedra is handled.
+int build_patch_table(sod_gpu_ctx *c, const std::vector<int> &conn, std::vector<int> &pt) {
+  const int P = c->P, N1 = c->N1, N = c->N, F2 = N1 * N1, NP = N + 6 * F2;
+  const long long E = c->nelem;
+  auto tid = [&](const int *ijk) { return ijk[0] + N1 * (ijk[1] + N1 * ijk[2]); };
+  auto face_ijk = [&](int f, int a, int b, int *ijk) {
+    const int d = f / 2, d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
+    ijk[d] = (f % 2) ? P : 0;
+    ijk[d1] = a;
+    ijk[d2] = b;
+  };
+  struct FaceKey {
+    std::array<int, 4> k;
+    long long e;
+    int f;
+  };
+  std::vector<FaceKey> keys((size_t)E * 6);
+  for (long long e = 0; e < E; ++e)
+    for (int f = 0; f < 6; ++f) {
+      FaceKey &fk = keys[e * 6 + f];
+      int q = 0, ijk[3];
+      for (int a = 0; a <= P; a += P)
+        for (int b = 0; b <= P; b += P) {
+          face_ijk(f, a, b, ijk);
+          fk.k[q++] = conn[e * N + tid(ijk)];
+        }
+      std::sort(fk.k.begin(), fk.k.end());
+      fk.e = e;
+      fk.f = f;
+    }
+  std::sort(keys.begin(), keys.end(), [](const FaceKey &x, const FaceKey &y) {
+    return x.k != y.k ? x.k < y.k : (x.e != y.e ? x.e < y.e : x.f < y.f);
+  });
+  std::vector<long long> nbr((size_t)E * 6);
+  for (long long i = 0; i < E * 6; ++i) nbr[i] = i / 6;
+  for (size_t i = 0; i < keys.size();) {
+    size_t j = i + 1;
+    while (j < keys.size() && keys[j].k == keys[i].k) ++j;
+    if (j - i == 2) {
+      nbr[keys[i].e * 6 + keys[i].f] = keys[i + 1].e;
+      nbr[keys[i + 1].e * 6 + keys[i + 1].f] = keys[i].e;
+    }
+    i = j;
+  }
+  pt.assign((size_t)E * NP, -1);
+  for (long long e = 0; e < E; ++e) {
+    for (int t = 0; t < N; ++t) pt[e * NP + t] = conn[e * N + t];
+    for (int f = 0; f < 6; ++f) {
+      const long long e2 = nbr[e * 6 + f];
+      if (e2 == e) continue;
+      auto locate = [&](int a, int b, int *out) {
+        int ijk[3];
+        face_ijk(f, a, b, ijk);
+        const int g = conn[e * N + tid(ijk)];
+        for (int t = 0; t < N; ++t)
+          if (conn[e2 * N + t] == g) {
+            out[0] = t % N1; out[1] = (t / N1) % N1; out[2] = t / F2;
+            return true;
+          }
+        return false;
+      };
+      int c00[3], cP0[3], c0P[3];
+      if (!locate(0, 0, c00) || !locate(P, 0, cP0) || !locate(0, P, c0P))
+        return fail(SOD_GPU_EINVAL, "inconsistent face connectivity");
+      int dn = -1, ncst = 0;
+      for (int x = 0; x < 3; ++x)
+        if (c00[x] == cP0[x] && c00[x] == c0P[x]) { dn = x; ++ncst; }
+      if (ncst != 1 || (c00[dn] != 0 && c00[dn] != P)) return fail(SOD_GPU_EINVAL, "inconsistent face connectivity");
+      const int step = c00[dn] == 0 ? 1 : -1;
+      for (int b = 0; b <= P; ++b)
+        for (int a = 0; a <= P; ++a) {
+          int ijk2[3];
+          for (int x = 0; x < 3; ++x) ijk2[x] = c00[x] + (cP0[x] - c00[x]) / P * a + (c0P[x] - c00[x]) / P * b;
+          ijk2[dn] += step;
+          pt[e * NP + N + f * F2 + a + N1 * b] = conn[e2 * N + tid(ijk2)];
+        }
+    }
   }
   return 0;
 }
@@ -1488,96 +1591,102 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
   const long long E = c->nelem;
   if (!NT.ready) {
     NT.nparam = sod_gpu_precond_num_params(c);
-    NT.bwd_threads = P == 3 ? 256 : 128;
-    NT.nblk_bwd = 148;
-    const int nact = P == 3 ? NetDims<3>::NACT : NetDims<4>::NACT;
+    NT.NP = P == 3 ? NetDims<3>::NP : NetDims<4>::NP;
+    const size_t NPt = (size_t)E * NT.NP;
     if ((rc = c->alloc(&NT.params, NT.nparam)) || (rc = c->alloc(&NT.m1, NT.nparam)) ||
         (rc = c->alloc(&NT.m2, NT.nparam)) || (rc = c->alloc(&NT.grad, NT.nparam)) ||
-        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.wts, (size_t)E * N)) ||
-        (rc = c->alloc(&NT.emean, (size_t)E)) || (rc = c->alloc(&NT.act, (size_t)E * nact)) ||
-        (rc = c->alloc(&NT.nbr, (size_t)E * 6)) || (rc = c->alloc(&NT.tmp1, (size_t)c->npoin)) ||
-        (rc = c->alloc(&NT.tmp2, (size_t)c->npoin)) || (rc = c->alloc(&NT.zf, (size_t)c->npoin)))
+        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.pt, NPt)) ||
+        (rc = c->alloc(&NT.pptr, (size_t)c->npoin + 1)) || (rc = c->alloc(&NT.pslot, NPt)) ||
+        (rc = c->alloc(&NT.feat, (size_t)E * NET_F)) || (rc = c->alloc(&NT.gains, (size_t)E * NET_K)) ||
+        (rc = c->alloc(&NT.Dh, (size_t)c->npoin)) || (rc = c->alloc(&NT.tmp1, (size_t)c->npoin)) ||
+        (rc = c->alloc(&NT.tmp2, (size_t)c->npoin)))
       return rc;
-    const size_t smb = P == 3 ? bwd_smem<3>(8) : bwd_smem<4>(4);
     if (P == 3) {
-      CUDA_TRY(cudaFuncSetAttribute(k_net_bwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+      using D = NetDims<3>;
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
+      CUDA_TRY(cudaFuncSetAttribute(k_mlp_bwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * D::NMLP * 4));
     } else {
-      CUDA_TRY(cudaFuncSetAttribute(k_net_bwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb));
+      using D = NetDims<4>;
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
+      CUDA_TRY(cudaFuncSetAttribute(k_mlp_bwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * D::NMLP * 4));
     }
-    // connectivity back on the host: face neighbours and assembly weights
-    std::vector<int> conn((size_t)E * N), lel(c->npoin, 0);
+    // patch table and its node-centric CSR (slots in increasing (e, j) order)
+    std::vector<int> conn((size_t)E * N), pt;
     CUDA_TRY(cudaMemcpy(conn.data(), c->conn, conn.size() * 4, cudaMemcpyDeviceToHost));
+    if ((rc = build_patch_table(c, conn, pt))) return rc;
+    std::vector<int> pptr(c->npoin + 1, 0), pslot(pt.size());
+    for (int v : pt)
+      if (v >= 0) pptr[v + 1]++;
+    for (long long n = 0; n < c->npoin; ++n) pptr[n + 1] += pptr[n];
+    std::vector<int> fill(pptr.begin(), pptr.end() - 1);
+    for (size_t i = 0; i < pt.size(); ++i)
+      if (pt[i] >= 0) pslot[fill[pt[i]]++] = (int)i;
+    CUDA_TRY(cudaMemcpy(NT.pt, pt.data(), pt.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(NT.pptr, pptr.data(), pptr.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(NT.pslot, pslot.data(), (size_t)pptr[c->npoin] * 4, cudaMemcpyHostToDevice));
+    // geometry features, the last two relative to their mesh mean
+    dispatch(c, [&](auto L) {
+      using LL = decltype(L);
+      k_elem_features<LL::P_><<<nblk(E, 8), 256, 0, c->stream>>>(c->md(), NT.tmp1);
+      return 0;
+    });
+    std::vector<double> raw((size_t)E * NET_F);
+    CUDA_TRY(cudaMemcpyAsync(raw.data(), NT.tmp1, raw.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double mean6 = 0.0, mean7 = 0.0;
+    for (long long e = 0; e < E; ++e) { mean6 += raw[e * NET_F + 6]; mean7 += raw[e * NET_F + 7]; }
+    mean6 /= (double)E;
+    mean7 /= (double)E;
+    std::vector<float> feat(raw.size());
     for (long long e = 0; e < E; ++e)
-      for (int t = 0; t < N; ++t) lel[conn[e * N + t]]++;
-    std::vector<float> w((size_t)E * N);
-    for (long long e = 0; e < E; ++e)
-      for (int t = 0; t < N; ++t) w[e * N + t] = 1.0f / (float)lel[conn[e * N + t]];
-    const int N1 = c->N1, Pm = P;
-    auto tid = [&](int i, int j, int k) { return i + N1 * (j + N1 * k); };
-    std::map<std::array<int, 4>, std::vector<std::pair<long long, int>>> faces;
-    for (long long e = 0; e < E; ++e)
-      for (int f = 0; f < 6; ++f) {
-        const int d = f / 2, v = (f % 2) ? Pm : 0;
-        std::array<int, 4> key;
-        int q = 0;
-        for (int a = 0; a <= Pm; a += Pm)
-          for (int b = 0; b <= Pm; b += Pm) {
-            int i = 0, j = 0, k = 0;
-            if (d == 0) { i = v; j = a; k = b; }
-            if (d == 1) { i = a; j = v; k = b; }
-            if (d == 2) { i = a; j = b; k = v; }
-            key[q++] = conn[e * N + tid(i, j, k)];
-          }
-        std::sort(key.begin(), key.end());
-        faces[key].push_back({e, f});
-      }
-    std::vector<int> nbr((size_t)E * 6);
-    for (long long e = 0; e < E; ++e)
-      for (int f = 0; f < 6; ++f) nbr[e * 6 + f] = (int)e;
-    for (auto &kv : faces) {
-      auto &v = kv.second;
-      if (v.size() == 2) {
-        nbr[v[0].first * 6 + v[0].second] = (int)v[1].first;
-        nbr[v[1].first * 6 + v[1].second] = (int)v[0].first;
-      }
-    }
-    CUDA_TRY(cudaMemcpy(NT.wts, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(NT.nbr, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice));
+      for (int q = 0; q < NET_F; ++q)
+        feat[e * NET_F + q] = (float)(raw[e * NET_F + q] - (q == 6 ? mean6 : (q == 7 ? mean7 : 0.0)));
+    CUDA_TRY(cudaMemcpy(NT.feat, feat.data(), feat.size() * 4, cudaMemcpyHostToDevice));
+    k_inv_sqrt_diag<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, c->cg.diag, NT.Dh);
     NT.ready = true;
   }
-  // seeded initial parameters: Xavier-uniform hidden layers, zero output layer
-  // (the network starts as Jacobi through its skip term)
+  // seeded initial parameters: small patch modes, zero skip exponent, Xavier
+  // hidden layers, zero output layer with unit gains: the map starts as Jacobi
   {
-    const int NIN = N + 6, H = NET_H;
+    const int NPn = NT.NP, H = NET_H, K = NET_K, Fn = NET_F;
+    const int o_alpha = K * NPn, o_w1 = o_alpha + 1, o_b1 = o_w1 + Fn * H, o_w2 = o_b1 + H, o_b2 = o_w2 + H * H,
+              o_w3 = o_b2 + H, o_b3 = o_w3 + H * K;
     std::vector<float> p(NT.nparam, 0.f);
     std::mt19937_64 rng(seed);
     std::uniform_real_distribution<float> U(-1.f, 1.f);
-    const float a1 = std::sqrt(6.f / (NIN + H)), a2 = std::sqrt(6.f / (H + H));
-    for (int i = 0; i < NIN * H; ++i) p[i] = a1 * U(rng);
-    const int o_w2 = NIN * H + H;
+    for (int i = 0; i < K * NPn; ++i) p[i] = 1.7e-3f * U(rng);
+    const float a1 = std::sqrt(6.f / (Fn + H)), a2 = std::sqrt(6.f / (H + H));
+    for (int i = 0; i < Fn * H; ++i) p[o_w1 + i] = a1 * U(rng);
     for (int i = 0; i < H * H; ++i) p[o_w2 + i] = a2 * U(rng);
+    for (int i = 0; i < K; ++i) p[o_b3 + i] = 0.54132485f;  // softplus^-1(1)
     CUDA_TRY(cudaMemcpy(NT.params, p.data(), p.size() * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(NT.m1, 0, (size_t)NT.nparam * 4));
     CUDA_TRY(cudaMemset(NT.m2, 0, (size_t)NT.nparam * 4));
     NT.step = 0;
+    NT.gains_ok = false;
+    NT.rs_state = 0x9e3779b97f4a7c15ULL ^ seed;
   }
   if (harvest_capacity > 0 && harvest_capacity != NT.cap) {
     if ((rc = c->alloc(&NT.hr, (size_t)harvest_capacity * c->npoin)) ||
         (rc = c->alloc(&NT.he, (size_t)harvest_capacity * c->npoin)) ||
-        (rc = c->alloc(&NT.xsnap, (size_t)16 * c->npoin)))
+        (!NT.xsnap && (rc = c->alloc(&NT.xsnap, (size_t)16 * c->npoin))))
       return rc;
     CUDA_TRY(cudaMemset(NT.hr, 0, (size_t)harvest_capacity * c->npoin * 4));
     CUDA_TRY(cudaMemset(NT.he, 0, (size_t)harvest_capacity * c->npoin * 4));
     NT.cap = harvest_capacity;
-    NT.count = NT.next = 0;
+    NT.count = 0;
+    NT.offered = 0;
     NT.eAe.assign(harvest_capacity, 1.0);
   }
-  return 0;
+  return c->finish();
 }
 
 int sod_gpu_precond_set_params(sod_gpu_ctx *c, const float *host_params, int n) {
   if (!c || !c->net.ready || !host_params || n != c->net.nparam) return fail(SOD_GPU_EINVAL, "bad argument");
   CUDA_TRY(cudaMemcpy(c->net.params, host_params, (size_t)n * 4, cudaMemcpyHostToDevice));
+  c->net.gains_ok = false;
   return 0;
 }
 
@@ -1591,7 +1700,6 @@ int sod_gpu_precond_apply(sod_gpu_ctx *c, const double *r, double *z) {
   if (!c || !r || !z) return fail(SOD_GPU_EINVAL, "bad argument");
   int rc;
   if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c))) return rc;
-  k_inv_diag64<<<nblk(c->npoin, 256), 256, 0, c->stream>>>((long long)c->npoin, c->cg.diag, c->cg.Minv);
   if ((rc = apply_precond(c, 1, r, z))) return rc;
   return c->finish();
 }
@@ -1599,8 +1707,6 @@ int sod_gpu_precond_apply(sod_gpu_ctx *c, const double *r, double *z) {
 int sod_gpu_precond_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double *loss, float *grad_host) {
   if (!c || !c->net.ready || !r || !e || !loss) return fail(SOD_GPU_EINVAL, "bad argument");
   auto &NT = c->net;
-  k_inv_diag64<<<nblk(c->npoin, 256), 256, 0, c->stream>>>((long long)c->npoin, c->cg.diag, c->cg.Minv);
-  // eAe
   lap<double>(c, e, NT.tmp2);
   dots<double, 1>(c, DotArgs<double, 1>{{e}, {NT.tmp2}, {nullptr}}, c->cg.dots + 5);
   double eAe;
@@ -1624,7 +1730,6 @@ int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64
   if (!c || !c->net.ready || steps < 0 || batch < 1 || batch > 16) return fail(SOD_GPU_EINVAL, "bad argument");
   auto &NT = c->net;
   if (NT.count < 1) return fail(SOD_GPU_EINVAL, "no harvested pairs to train on");
-  k_inv_diag64<<<nblk(c->npoin, 256), 256, 0, c->stream>>>((long long)c->npoin, c->cg.diag, c->cg.Minv);
   double *rd = c->cg.z1, *ed = c->cg.q;  // FP64 staging of one pair (solver scratch, idle here)
   std::mt19937_64 rng(seed);
   double last = 0.0;
@@ -1647,6 +1752,7 @@ int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64
     k_adam<<<nblk(NT.nparam, 256), 256, 0, c->stream>>>(NT.nparam, NT.nblk_bwd * batch, NT.part, NT.params, NT.m1,
                                                         NT.m2, lr, 0.9f, 0.999f, 1e-8f, bc1, bc2, 1.f / batch,
                                                         nullptr);
+    NT.gains_ok = false;
     last = sum / batch;
   }
   CUDA_TRY(cudaStreamSynchronize(c->stream));

@@ -1,7 +1,8 @@
-"""Learned preconditioner on the GPU: forward/backward kernels against the
-numpy restatement, and the gain of the trained network over Jacobi inside
-the FP64-certified flexible CG on pressure systems of an incompressible
-Taylor-Green run."""
+"""Learned preconditioner on the GPU: inference, forward and backward kernels
+against the numpy restatement (P=3 and P=4, shuffled element and node
+numbering), and the gain of the trained network over Jacobi inside the
+FP64-certified CG on pressure systems of an incompressible Taylor-Green
+run."""
 import ctypes as C
 
 import numpy as np
@@ -23,39 +24,53 @@ def gpu():
     return g
 
 
-def test_loss_and_gradient_match_oracle(gpu):
-    m = host.periodic_cube(3, 4, jitter=0.05, seed=6, ordering=1, elem_shuffle=True)
+def _random_params(P, seed):
+    rng = np.random.default_rng(seed)
+    off = PR.dims(P)[2]
+    p = rng.normal(0, 0.2, PR.num_params(P))
+    o, n = off["B"]
+    p[o:o + n] = rng.normal(0, 0.05, n)
+    return p.astype(np.float32)
+
+
+@pytest.mark.parametrize("porder", [3, 4])
+def test_loss_and_gradient_match_oracle(gpu, porder):
+    m = host.periodic_cube(porder, 4, jitter=0.05, seed=6, ordering=1, elem_shuffle=True)
     ctx = gpu.Context(m, gpu.default_phys())
     ctx.call("sod_gpu_precond_init", 7, 0)
     n = gpu.lib().sod_gpu_precond_num_params(ctx.h)
-    rng = np.random.default_rng(3)
-    params = rng.normal(0, 0.2, n).astype(np.float32)
+    assert n == PR.num_params(porder)
+    params = _random_params(porder, 3)
     ctx.call("sod_gpu_precond_set_params", params.ctypes.data_as(C.c_void_p), n)
     om = O.OracleMesh(m, np.float64)
     diag = torch.zeros(m.npoin, device="cuda")
     ctx.call("sod_gpu_eval_laplacian_diag", gpu.dptr(diag))
     w = m.lpoin_w - 1
-    Minv = np.zeros(m.npoin)
-    Minv[w] = 1.0 / diag.cpu().numpy()[w].astype(np.float64)
-    net = PR.Net(m, Minv)
+    net = PR.Net(m, diag.cpu().numpy())
+    rng = np.random.default_rng(3)
     e = np.zeros(m.npoin)
     e[w] = rng.normal(size=w.size)
     r = O.laplacian(om, e)
-    ref_loss, ref_grad = net.loss_grad(params.astype(np.float64), r, e, lambda v: O.laplacian(om, v))
-    loss = C.c_double()
-    grad = np.zeros(n, np.float32)
     dr, de = torch.from_numpy(r).cuda(), torch.from_numpy(e).cuda()
-    ctx.call("sod_gpu_precond_loss_grad", gpu.dptr(dr), gpu.dptr(de), C.byref(loss), grad.ctypes.data_as(C.c_void_p))
-    print("loss", loss.value, ref_loss)
-    assert abs(loss.value - ref_loss) / ref_loss < 1e-4
-    err = np.linalg.norm(grad - ref_grad) / np.linalg.norm(ref_grad)
-    print("grad rel L2", err)
-    assert err < 1e-3
-    # forward: apply == oracle forward
+    # inference
     z = torch.zeros(m.npoin, dtype=torch.float64, device="cuda")
     ctx.call("sod_gpu_precond_apply", gpu.dptr(dr), gpu.dptr(z))
     zr, _ = net.forward(params.astype(np.float64), r)
-    assert np.linalg.norm(z.cpu().numpy()[w] - zr[w]) / np.linalg.norm(zr[w]) < 1e-5
+    zerr = np.linalg.norm(z.cpu().numpy()[w] - zr[w]) / np.linalg.norm(zr[w])
+    print("apply rel L2", zerr)
+    assert zerr < 1e-5
+    # loss and gradient
+    ref_loss, ref_grad = net.loss_grad(params.astype(np.float64), r, e, lambda v: O.laplacian(om, v))
+    loss = C.c_double()
+    grad = np.zeros(n, np.float32)
+    ctx.call("sod_gpu_precond_loss_grad", gpu.dptr(dr), gpu.dptr(de), C.byref(loss), grad.ctypes.data_as(C.c_void_p))
+    print("loss", loss.value, ref_loss)
+    assert abs(loss.value - ref_loss) / ref_loss < 1e-4
+    off = PR.dims(porder)[2]
+    for name, (o, k) in off.items():
+        err = np.linalg.norm(grad[o:o + k] - ref_grad[o:o + k]) / max(np.linalg.norm(ref_grad[o:o + k]), 1e-30)
+        print("grad", name, "rel L2", err)
+        assert err < 1e-3, name
     ctx.close()
 
 
@@ -79,7 +94,7 @@ def test_trained_network_beats_jacobi(gpu):
         assert st.res_rel < 1e-8
     assert gpu.lib().sod_gpu_precond_harvest_count(ctx.h) > 10
     loss = C.c_float()
-    ctx.call("sod_gpu_precond_train", 300, 8, 2e-3, 5, C.byref(loss))
+    ctx.call("sod_gpu_precond_train", 300, 8, 3e-3, 5, C.byref(loss))
     print("Jacobi iterations", its_j, "final training loss", loss.value)
     # the next pressure system, solved from the same zero initial guess by both
     uu = torch.zeros(3 * N, device="cuda")
@@ -103,5 +118,5 @@ def test_trained_network_beats_jacobi(gpu):
         out[name] = (st.iterations, st.res_rel, st.fallback, st.seconds)
     print("jacobi:", out["jacobi"], " learned:", out["learned"])
     assert out["learned"][1] < 1e-8 and out["learned"][2] == 0
-    assert out["learned"][0] < out["jacobi"][0]
+    assert out["learned"][0] < 0.6 * out["jacobi"][0]
     ctx.close()
