@@ -206,7 +206,7 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
         c = ctxs[0] if kind == 1 else ctxs[1]
         it, ms, rmax, fb = [], [], 0.0, 0
         for k in range(compare_steps):
-            o = gpu.SolveOpts(50000, 1e-8, kind, 200, 0, 4)
+            o = gpu.SolveOpts(50000, 1e-8, kind, 200, 0)
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
             it.append(st.iterations)
             ms.append(st.seconds * 1e3)

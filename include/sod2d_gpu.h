@@ -171,15 +171,15 @@ int sod_gpu_full_convec_ijk_incomp(sod_gpu_ctx *ctx, const float *u, const float
 int sod_gpu_conjgrad_pressure(sod_gpu_ctx *ctx, const float *Rp0, float *R, int maxIter, double tol,
                               int *iters, double *res_rel);
 
-/* Pressure solve to an FP64-certified tolerance on FP64 vectors with the
- * FP64 Laplacian.  Preconditioner 0 = Jacobi with the reference's
- * Polak-Ribiere CG; 1 = the learned element-patch network
- * (sod_gpu_precond_*) inside a truncated flexible CG (each new direction is
- * A-orthogonalised against the last `truncation` ones), falling back to
- * Jacobi when the residual stagnates.  b is made mean-free over working
- * nodes (the periodic Laplacian's null space).  Convergence is declared
- * only when the true residual ||b - A x|| / ||b||, recomputed in FP64,
- * is below tol. */
+/* Pressure solve to an FP64-certified tolerance: flexible (Polak-Ribiere)
+ * preconditioned CG, the reference's form, on FP64 vectors with the FP64
+ * Laplacian.  Preconditioner 0 = Jacobi; 1 = the learned element-patch
+ * preconditioner (sod_gpu_precond_*), falling back to Jacobi when the
+ * residual stagnates.  The iteration scalars stay on the device and the
+ * host reads them once per batch of iterations.  b is made mean-free over
+ * working nodes (the periodic Laplacian's null space).  Convergence is
+ * declared only when the true residual ||b - A x|| / ||b||, recomputed in
+ * FP64, is below tol. */
 typedef struct {
   int max_iter;
   double tol;
@@ -187,8 +187,6 @@ typedef struct {
   int stagnation_window; /* iterations without a 2x residual drop -> fallback */
   int harvest;         /* 1: record (residual, error) pairs of this solve for
                           training the learned preconditioner             */
-  int truncation;      /* learned path: directions kept by the truncated
-                          flexible CG (0 = default 4, max 7)              */
 } sod_solve_opts_t;
 typedef struct {
   int iterations;

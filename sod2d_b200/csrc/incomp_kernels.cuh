@@ -12,8 +12,9 @@ namespace sod {
 // Writes one V per element node into slots (width 1).
 template <int P, int EPB, class V>
 __global__ void __launch_bounds__(EPB *Cfg<P>::NT)
-k_lap_elem(MeshDev m, const V *__restrict__ p, V *__restrict__ slots) {
+k_lap_elem(MeshDev m, const V *__restrict__ p, V *__restrict__ slots, const int *__restrict__ stop = nullptr) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
+  if (stop && *stop) return;
   __shared__ V sm[EPB][4][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
   const long long e = (long long)blockIdx.x * EPB + el;
@@ -251,4 +252,288 @@ __global__ void k_dot_final(int nd, const double *__restrict__ part, double *__r
   }
 }
 
+// ---- device-resident preconditioned CG -------------------------------------
+// Scalars of the iteration kept in device memory between launches, so that
+// the host only reads them once per batch of iterations.  Every iteration
+// kernel returns at once when status != 0.
+struct CgScal {
+  double rz;     // r . z of the current residual
+  double pq;     // p . A p
+  double alpha, beta;
+  double rr;     // ||r||^2 after the last update
+  double thr2;   // (tol ||b||)^2
+  int iter;      // iterations done in this solve
+  int status;    // 0 running, 1 converged (recursive residual), 2 breakdown, 3 non-finite
+};
+
+constexpr int CG_THREADS = 256, CG_U = 4;
+
+// Node loops of the CG kernels handle several nodes per thread and issue all
+// their loads before any store, so that each thread keeps several memory
+// round trips in flight.
+inline unsigned cg_blocks(long long n, int u) {
+  const long long b = (n + (long long)CG_THREADS * u - 1) / ((long long)CG_THREADS * u);
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+// Deterministic grid-wide sum of ND doubles: each block reduces its values
+// in a fixed order and stores one partial; the last block to take a ticket
+// adds the partials in block order.  Returns true (in every thread of that
+// block only) with tot filled; the ticket is reset for the next launch.
+template <int ND>
+__device__ bool grid_sum(double (&v)[ND], double *__restrict__ part, unsigned *ticket, double (&tot)[ND]) {
+  __shared__ double sh[ND][32];
+  __shared__ bool last;
+  const int lane = threadIdx.x % 32, warp = threadIdx.x / 32, nw = blockDim.x / 32;
+#pragma unroll
+  for (int d = 0; d < ND; ++d)
+    for (int o = 16; o > 0; o >>= 1) v[d] += __shfl_xor_sync(0xffffffffu, v[d], o);
+  if (lane == 0)
+    for (int d = 0; d < ND; ++d) sh[d][warp] = v[d];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int d = 0; d < ND; ++d) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += sh[d][w];
+      part[d * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) s += __ldcg(part + d * gridDim.x + b);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __syncthreads();
+    if (lane == 0) sh[d][warp] = s;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += sh[d][w];
+    tot[d] = t;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+// q = assembled Laplacian slots (Kahan, as k_gather1) with the p.q partials;
+// the last block sets alpha = rz / pq.
+__global__ void __launch_bounds__(CG_THREADS)
+k_cg_q(MeshDev m, const double *__restrict__ slots, const double *__restrict__ p, double *__restrict__ q,
+       CgScal *S, double *__restrict__ part, unsigned *ticket) {
+  if (S->status) return;
+  constexpr int U = 2, MS = 8;  // nodes per thread, slots loaded ahead per node
+  double v[1] = {0.0};
+  for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < m.npoin;
+       base += (long long)gridDim.x * blockDim.x * U) {
+    int b[U], en[U];
+    double pn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long n = base + (long long)u * blockDim.x;
+      b[u] = en[u] = 0;
+      pn[u] = 0.0;
+      if (n < m.npoin) { b[u] = m.slot_ptr[n]; en[u] = m.slot_ptr[n + 1]; pn[u] = p[n]; }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long n = base + (long long)u * blockDim.x;
+      if (n >= m.npoin) continue;
+      double sum = 0.0, cmp = 0.0;
+      for (int s0 = b[u]; s0 < en[u]; s0 += MS) {
+        int id[MS];
+        double y[MS];
+#pragma unroll
+        for (int k = 0; k < MS; ++k) id[k] = s0 + k < en[u] ? m.slot_idx[s0 + k] : -1;
+#pragma unroll
+        for (int k = 0; k < MS; ++k) y[k] = id[k] >= 0 ? slots[id[k]] : 0.0;
+#pragma unroll
+        for (int k = 0; k < MS; ++k) {
+          if (id[k] < 0) break;
+          const double yy = y[k] - cmp;
+          const double tt = sum + yy;
+          cmp = (tt - sum) - yy;
+          sum = tt;
+        }
+      }
+      q[n] = sum;
+      if (b[u] != en[u]) v[0] += pn[u] * sum;
+    }
+  }
+  double tot[1];
+  if (grid_sum<1>(v, part, ticket, tot) && threadIdx.x == 0) {
+    S->pq = tot[0];
+    if (!isfinite(tot[0])) {
+      S->status = 3;
+    } else if (!(tot[0] > 0.0)) {
+      S->status = 2;
+    } else {
+      S->alpha = S->rz / tot[0];
+    }
+  }
+}
+
+// x += alpha p ; r -= alpha q ; with JAC also z = Minv r (reading the old z),
+// otherwise, when uf is given, uf = (float)(Dh r); the last block records
+// ||r||^2, detects convergence and, with JAC, sets the Polak-Ribiere
+// beta = r.(z - z_old) / rz_old.
+template <bool JAC>
+__global__ void __launch_bounds__(CG_THREADS)
+k_cg_update(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ p,
+            const double *__restrict__ q, const double *__restrict__ Minv, double *__restrict__ x,
+            double *__restrict__ r, double *__restrict__ z, CgScal *S, double *__restrict__ hist, int hist_cap,
+            double *__restrict__ part, unsigned *ticket, const double *__restrict__ Dh = nullptr,
+            float *__restrict__ uf = nullptr) {
+  if (S->status) return;
+  constexpr int U = CG_U;
+  const double a = S->alpha;
+  double v[3] = {0.0, 0.0, 0.0};
+  for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < npoin_w;
+       base += (long long)gridDim.x * blockDim.x * U) {
+    int id[U];
+    double pv[U], qv[U], xv[U], rv[U], mv[U], zv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long t = base + (long long)u * blockDim.x;
+      id[u] = t < npoin_w ? lpoin_w[t] : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (id[u] < 0) continue;
+      const int i = id[u];
+      pv[u] = p[i]; qv[u] = q[i]; xv[u] = x[i]; rv[u] = r[i];
+      if (JAC) { mv[u] = Minv[i]; zv[u] = z[i]; }
+      if (!JAC && uf) mv[u] = Dh[i];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (id[u] < 0) continue;
+      const int i = id[u];
+      x[i] = xv[u] + a * pv[u];
+      const double rn = rv[u] - a * qv[u];
+      r[i] = rn;
+      v[0] += rn * rn;
+      if (JAC) {
+        const double zn = rn * mv[u];
+        z[i] = zn;
+        v[1] += rn * zn;
+        v[2] += rn * zv[u];
+      } else if (uf) {
+        uf[i] = (float)(mv[u] * rn);  // D^-1/2 r for the learned preconditioner
+      }
+    }
+  }
+  double tot[3];
+  if (grid_sum<3>(v, part, ticket, tot) && threadIdx.x == 0) {
+    const int it = S->iter + 1;
+    S->iter = it;
+    S->rr = tot[0];
+    hist[(it - 1) % hist_cap] = tot[0];
+    if (!isfinite(tot[0])) {
+      S->status = 3;
+    } else if (tot[0] < S->thr2) {
+      S->status = 1;
+    }
+    if (JAC) {
+      S->beta = (tot[1] - tot[2]) / S->rz;
+      S->rz = tot[1];
+    }
+  }
+}
+
+// Learned preconditioner: z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of
+// the node's patch slots) (as k_patch_gather), with the partials r.z and
+// r.z_old; the last block sets beta and rz.
+__global__ void __launch_bounds__(CG_THREADS)
+k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const int *__restrict__ pslot,
+             const float *__restrict__ slots, const double *__restrict__ r, const double *__restrict__ Dh,
+             const float *__restrict__ prm, int o_alpha, double *__restrict__ z, CgScal *S,
+             double *__restrict__ part, unsigned *ticket) {
+  if (S->status) return;
+  constexpr int U = 2, MS = 8;
+  const double gam = exp((double)prm[o_alpha]);
+  double v[2] = {0.0, 0.0};
+  for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < npoin;
+       base += (long long)gridDim.x * blockDim.x * U) {
+    int b[U], en[U];
+    double dv[U], rv[U], zo[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long n = base + (long long)u * blockDim.x;
+      b[u] = en[u] = 0;
+      if (n < npoin) {
+        b[u] = pptr[n]; en[u] = pptr[n + 1];
+        dv[u] = Dh[n]; rv[u] = r[n]; zo[u] = z[n];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (b[u] == en[u]) continue;
+      const long long n = base + (long long)u * blockDim.x;
+      double acc = 0.0;
+      for (int s0 = b[u]; s0 < en[u]; s0 += MS) {
+        int id[MS];
+        float y[MS];
+#pragma unroll
+        for (int k = 0; k < MS; ++k) id[k] = s0 + k < en[u] ? pslot[s0 + k] : -1;
+#pragma unroll
+        for (int k = 0; k < MS; ++k) y[k] = id[k] >= 0 ? slots[id[k]] : 0.f;
+#pragma unroll
+        for (int k = 0; k < MS; ++k) acc += (double)y[k];
+      }
+      const double zn = dv[u] * (gam * dv[u] * rv[u] + acc);
+      z[n] = zn;
+      v[0] += rv[u] * zn;
+      v[1] += rv[u] * zo[u];
+    }
+  }
+  double tot[2];
+  if (grid_sum<2>(v, part, ticket, tot) && threadIdx.x == 0) {
+    S->beta = (tot[0] - tot[1]) / S->rz;
+    S->rz = tot[0];
+    if (!isfinite(S->beta)) S->status = 3;
+  }
+}
+
+// p = z + beta p
+__global__ void __launch_bounds__(CG_THREADS)
+k_cg_dir(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ z, double *__restrict__ p,
+         const CgScal *S) {
+  if (S->status) return;
+  constexpr int U = CG_U;
+  const double bt = S->beta;
+  for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < npoin_w;
+       base += (long long)gridDim.x * blockDim.x * U) {
+    int id[U];
+    double zv[U], pv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long t = base + (long long)u * blockDim.x;
+      id[u] = t < npoin_w ? lpoin_w[t] : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (id[u] >= 0) { zv[u] = z[id[u]]; pv[u] = p[id[u]]; }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (id[u] >= 0) p[id[u]] = zv[u] + bt * pv[u];
+  }
+}
+
+// harvest snapshot of the iterate and residual (skipped once stopped)
+__global__ void k_cg_snapshot(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ x,
+                              const double *__restrict__ r, double *__restrict__ xs, float *__restrict__ rs,
+                              const CgScal *S) {
+  if (S->status) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npoin_w; t += gridDim.x * blockDim.x) {
+    const int i = lpoin_w[t];
+    xs[i] = x[i];
+    rs[i] = (float)r[i];
+  }
+}
+
 }  // namespace sod
+

@@ -119,22 +119,34 @@ __device__ void stage_B(const float *__restrict__ prm, float *BT, float *Bk) {
     }
 }
 
-// Gather D^-1/2 v over the patches of EPW elements into xs[EPW][NPP].
+// Gather D^-1/2 v over the patches of EPW elements into xs[EPW][NPP]; per
+// element the lane's slot indices are loaded first, then their values.
 template <int P>
 __device__ __forceinline__ void gather_patch(long long e0, long long nelem, const int *__restrict__ pt,
                                              const double *__restrict__ v, const double *__restrict__ Dh, float *xs,
                                              int lane) {
   using D = NetDims<P>;
+  constexpr int JN = (D::NPP + 31) / 32;
 #pragma unroll
   for (int el = 0; el < D::EPW; ++el) {
     const long long e = e0 + el;
-    for (int j = lane; j < D::NPP; j += 32) {
-      float x = 0.f;
-      if (e < nelem && j < D::NP) {
-        const int idx = pt[e * D::NP + j];
-        if (idx >= 0) x = (float)(Dh[idx] * v[idx]);
-      }
-      xs[el * D::NPP + j] = x;
+    int id[JN];
+#pragma unroll
+    for (int q = 0; q < JN; ++q) {
+      const int j = lane + 32 * q;
+      id[q] = (e < nelem && j < D::NP) ? pt[e * D::NP + j] : -1;
+    }
+    double dv[JN], vv[JN];
+#pragma unroll
+    for (int q = 0; q < JN; ++q) {
+      dv[q] = 0.0;
+      vv[q] = 0.0;
+      if (id[q] >= 0) { dv[q] = Dh[id[q]]; vv[q] = v[id[q]]; }
+    }
+#pragma unroll
+    for (int q = 0; q < JN; ++q) {
+      const int j = lane + 32 * q;
+      if (j < D::NPP) xs[el * D::NPP + j] = (float)(dv[q] * vv[q]);
     }
   }
 }
@@ -198,6 +210,159 @@ k_patch_apply(long long nelem, const int *__restrict__ pt, const double *__restr
 #pragma unroll
       for (int el = 0; el < EPW; ++el)
         if (e0 + el < nelem) slots[(e0 + el) * D::NP + j] = o[el];
+    }
+    __syncwarp();
+  }
+}
+
+// ---- tensor-core inference (mma.sync m16n8k8, TF32 operands, FP32 accumulate)
+// Each warp applies the patch operator to 16 elements at a time:
+//   H[16 x K] = X[16 x NP] B^T,  Y = gains * H,  O[16 x NP] = Y B.
+// Operands are staged in shared memory with row strides chosen so that the
+// fragment loads are free of bank conflicts.
+template <int P>
+struct TcDims {
+  using D = NetDims<P>;
+  static constexpr int KP = (D::NP + 7) / 8 * 8;                   // slots padded to the mma k/n step
+  static constexpr int S1 = KP + 4;                                // B as [mode][slot]: stride = 4 mod 8
+  static constexpr int S2 = KP + ((8 - KP % 16) + 16) % 16;        // B as [mode][slot]: stride = 8 or 24 mod 32
+  static constexpr int SX = KP + 4;                                // X tile [16][SX]
+  static constexpr int SY = NET_K + 4;                             // Y tile [16][SY]
+  static constexpr int WARPS = 4;
+  static constexpr size_t smem() { return (size_t)(NET_K * S1 + NET_K * S2 + WARPS * 16 * (SX + SY)) * 4; }
+};
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// uf = (float)(D^-1/2 r) over the working nodes
+__global__ void k_scale_f32(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
+                            const double *__restrict__ Dh, float *__restrict__ uf) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  uf[i] = (float)(Dh[i] * r[i]);
+}
+
+template <int P>
+__global__ void __launch_bounds__(128)
+k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const float *__restrict__ uf,
+                 const float *__restrict__ prm, const float *__restrict__ gains, float *__restrict__ slots,
+                 const int *__restrict__ stop) {
+  using D = NetDims<P>;
+  using T = TcDims<P>;
+  constexpr int NP = D::NP, KP = T::KP, K = NET_K, JN = (KP + 31) / 32, NT2 = KP / 8;
+  if (stop && *stop) return;
+  extern __shared__ __align__(16) float smem[];
+  float *B1 = smem, *B2 = B1 + K * T::S1;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  float *X = B2 + K * T::S2 + warp * 16 * (T::SX + T::SY), *Y = X + 16 * T::SX;
+  for (int i = threadIdx.x; i < K * KP; i += blockDim.x) {
+    const int k = i / KP, j = i % KP;
+    const float b = j < NP ? prm[D::O_B + k * NP + j] : 0.f;
+    B1[k * T::S1 + j] = b;
+    B2[k * T::S2 + j] = b;
+  }
+  __syncthreads();
+  const int g = lane >> 2, t = lane & 3;
+  const long long ngroups = (nelem + 15) / 16;
+  for (long long grp = (long long)blockIdx.x * T::WARPS + warp; grp < ngroups;
+       grp += (long long)gridDim.x * T::WARPS) {
+    const long long e0 = grp * 16;
+    // gather X = D^-1/2 r over the 16 patches (indices first, then values)
+#pragma unroll 1
+    for (int r0 = 0; r0 < 16; r0 += 4) {
+      int id[4][JN];
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+        for (int q = 0; q < JN; ++q) {
+          const long long e = e0 + r0 + rr;
+          const int j = lane + 32 * q;
+          id[rr][q] = (e < nelem && j < NP) ? pt[e * NP + j] : -1;
+        }
+      float xv[4][JN];
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+        for (int q = 0; q < JN; ++q) xv[rr][q] = id[rr][q] >= 0 ? uf[id[rr][q]] : 0.f;
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr)
+#pragma unroll
+        for (int q = 0; q < JN; ++q) {
+          const int j = lane + 32 * q;
+          if (j < KP) X[(r0 + rr) * T::SX + j] = xv[rr][q];
+        }
+    }
+    __syncwarp();
+    // H = X B^T : 4 n-tiles of 8 modes, KP/8 k-steps
+    float h[4][4];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) h[nt][q] = 0.f;
+#pragma unroll 4
+    for (int k0 = 0; k0 < KP; k0 += 8) {
+      const uint32_t a0 = __float_as_uint(X[g * T::SX + k0 + t]);
+      const uint32_t a1 = __float_as_uint(X[(g + 8) * T::SX + k0 + t]);
+      const uint32_t a2 = __float_as_uint(X[g * T::SX + k0 + t + 4]);
+      const uint32_t a3 = __float_as_uint(X[(g + 8) * T::SX + k0 + t + 4]);
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const uint32_t b0 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t]);
+        const uint32_t b1 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t + 4]);
+        mma_tf32(h[nt], a0, a1, a2, a3, b0, b1);
+      }
+    }
+    // Y = gains * H
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const int col = nt * 8 + 2 * t;
+      const long long ea = e0 + g, eb = e0 + g + 8;
+      const float2 sa = ea < nelem ? *reinterpret_cast<const float2 *>(gains + ea * K + col) : make_float2(0.f, 0.f);
+      const float2 sb = eb < nelem ? *reinterpret_cast<const float2 *>(gains + eb * K + col) : make_float2(0.f, 0.f);
+      Y[g * T::SY + col] = sa.x * h[nt][0];
+      Y[g * T::SY + col + 1] = sa.y * h[nt][1];
+      Y[(g + 8) * T::SY + col] = sb.x * h[nt][2];
+      Y[(g + 8) * T::SY + col + 1] = sb.y * h[nt][3];
+    }
+    __syncwarp();
+    uint32_t a[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const int k0 = kk * 8;
+      a[kk][0] = __float_as_uint(Y[g * T::SY + k0 + t]);
+      a[kk][1] = __float_as_uint(Y[(g + 8) * T::SY + k0 + t]);
+      a[kk][2] = __float_as_uint(Y[g * T::SY + k0 + t + 4]);
+      a[kk][3] = __float_as_uint(Y[(g + 8) * T::SY + k0 + t + 4]);
+    }
+    // O = Y B : KP/8 n-tiles of 8 slots, 4 k-steps
+#pragma unroll 2
+    for (int nt = 0; nt < NT2; ++nt) {
+      float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        const int k0 = kk * 8;
+        const uint32_t b0 = __float_as_uint(B2[(k0 + t) * T::S2 + nt * 8 + g]);
+        const uint32_t b1 = __float_as_uint(B2[(k0 + t + 4) * T::S2 + nt * 8 + g]);
+        mma_tf32(o, a[kk][0], a[kk][1], a[kk][2], a[kk][3], b0, b1);
+      }
+      const int col = nt * 8 + 2 * t;
+      const long long ea = e0 + g, eb = e0 + g + 8;
+      if (ea < nelem) {
+        if (col < NP) slots[ea * NP + col] = o[0];
+        if (col + 1 < NP) slots[ea * NP + col + 1] = o[1];
+      }
+      if (eb < nelem) {
+        if (col < NP) slots[eb * NP + col] = o[2];
+        if (col + 1 < NP) slots[eb * NP + col + 1] = o[3];
+      }
     }
     __syncwarp();
   }

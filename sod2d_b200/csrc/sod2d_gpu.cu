@@ -59,6 +59,7 @@ struct sod_gpu_ctx {
   float *slotsA = nullptr, *slotsB = nullptr, *proj12 = nullptr, *mue_t = nullptr, *musgs_t = nullptr;
   size_t bytes = 0;
   std::vector<void *> allocs;
+  std::vector<void *> host_allocs;  // pinned host memory
   // analysis / entropy-viscosity support
   int *is_work = nullptr;
   float *Ngp_t = nullptr;  // [g][a] tensor order
@@ -70,7 +71,10 @@ struct sod_gpu_ctx {
     float *x32, *r32, *p32, *q32, *z032, *z132, *b32;          // reference-arithmetic CG
     double *x, *r, *p, *q, *z0, *z1, *b, *Minv;                // FP64 CG
     double *part, *dots;                                        // reductions
-    double *Pm = nullptr, *Qm = nullptr;                        // truncated-FCG direction ring (7 x npoin each)
+    CgScal *S = nullptr, *S_h = nullptr;                        // device-resident CG scalars (+ pinned host copy)
+    double *hist = nullptr, *hist_h = nullptr;                  // ||r||^2 per iteration (ring)
+    unsigned *ticket = nullptr;                                 // grid-sum ticket
+    double *gpart = nullptr;                                    // grid-sum block partials
   } cg;
   // learned preconditioner
   struct Net {
@@ -81,6 +85,7 @@ struct sod_gpu_ctx {
     float *feat = nullptr, *gains = nullptr;                  // [E][8], [E][32]
     float *X = nullptr, *W = nullptr, *Y = nullptr, *SA = nullptr, *dS = nullptr;  // training scratch
     double *Dh = nullptr;                                     // D^-1/2
+    float *uf = nullptr;                                      // (float) D^-1/2 r for tensor-core inference
     // harvested (r, e) pairs, FP32, reservoir-sampled, and e^T A e per pair
     int cap = 0, count = 0;
     long long offered = 0;
@@ -392,6 +397,7 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
 int sod_gpu_finalize(sod_gpu_ctx *ctx) {
   if (!ctx) return 0;
   for (void *p : ctx->allocs) cudaFree(p);
+  for (void *p : ctx->host_allocs) cudaFreeHost(p);
   delete ctx;
   return 0;
 }
@@ -635,6 +641,37 @@ int ensure_cg64(sod_gpu_ctx *c) {
   return 0;
 }
 
+constexpr int CG_HIST = 1024;
+
+int ensure_cg_loop(sod_gpu_ctx *c) {
+  auto &G = c->cg;
+  if (G.S) return 0;
+  int rc;
+  if ((rc = c->alloc(&G.S, 1)) || (rc = c->alloc(&G.hist, CG_HIST)) || (rc = c->alloc(&G.ticket, 1)) ||
+      (rc = c->alloc(&G.gpart, (size_t)3 * cg_blocks(c->npoin, 2))))
+    return rc;
+  CUDA_TRY(cudaMemset(G.ticket, 0, sizeof(unsigned)));
+  CUDA_TRY(cudaMemset(G.S, 0, sizeof(CgScal)));
+  void *h1 = nullptr, *h2 = nullptr;
+  CUDA_TRY(cudaMallocHost(&h1, sizeof(CgScal)));
+  CUDA_TRY(cudaMallocHost(&h2, sizeof(double) * CG_HIST));
+  G.S_h = (CgScal *)h1;
+  G.hist_h = (double *)h2;
+  c->host_allocs.push_back(h1);
+  c->host_allocs.push_back(h2);
+  return 0;
+}
+
+// start (or restart) of the device-resident CG: d = [r.z, r.r]
+__global__ void k_cg_start(CgScal *S, const double *__restrict__ d, double thr2, int iter) {
+  S->rz = d[0];
+  S->rr = d[1];
+  S->thr2 = thr2;
+  S->iter = iter;
+  S->alpha = S->beta = 0.0;
+  S->status = !isfinite(d[1]) ? 3 : (d[1] < thr2 ? 1 : 0);
+}
+
 __global__ void k_inv_diag64(long long n, const float *__restrict__ d, double *__restrict__ minv) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) minv[i] = d[i] != 0.f ? 1.0 / (double)d[i] : 0.0;
@@ -776,6 +813,7 @@ namespace {
 // ---- FP64 flexible CG with certified residual ----------------------------
 
 int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z);  // defined with the network
+int ensure_gains(sod_gpu_ctx *c);
 
 __global__ void k_d2f_w(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ a,
                         float *__restrict__ b);
@@ -810,23 +848,6 @@ __global__ void k_jacobi64(int npoin_w, const int *__restrict__ lpoin_w, const d
   z[i] = r[i] * Minv[i];
 }
 
-struct MultiAxpy {
-  int n;
-  const double *v[8];
-  double c[8];
-};
-
-// p = z + sum_j c_j v_j over working nodes
-__global__ void k_multi_axpy(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ z, MultiAxpy M,
-                             double *__restrict__ p) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npoin_w) return;
-  const int i = lpoin_w[t];
-  double a = z[i];
-  for (int j = 0; j < M.n; ++j) a += M.c[j] * M.v[j][i];
-  p[i] = a;
-}
-
 // r = b - q over working nodes
 __global__ void k_resid(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ b,
                         const double *__restrict__ q, double *__restrict__ r) {
@@ -843,8 +864,9 @@ extern "C" {
 int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const sod_solve_opts_t *opts,
                            sod_solve_stats_t *stats) {
   if (!c || !b_in || !x || !opts || opts->max_iter < 1 || !(opts->tol > 0)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (opts->precond != 0 && opts->precond != 1) return fail(SOD_GPU_EINVAL, "precond must be 0 or 1");
   int rc;
-  if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c))) return rc;
+  if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c)) || (rc = ensure_cg_loop(c))) return rc;
   auto &G = c->cg;
   const size_t N = c->npoin;
   const int nw = c->npoin_w;
@@ -869,16 +891,27 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
   double res = 0.0;
   const int window = opts->stagnation_window > 0 ? opts->stagnation_window : 50;
   auto &NT = c->net;
+  if (kind == 1) {
+    if (!NT.ready) return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
+    if ((rc = ensure_gains(c))) return rc;
+  }
+  // harvest snapshots (x_k, r_k) after k = 0..8, 16, 32, ... iterations
   const bool harvest = opts->harvest && NT.ready && NT.cap > 0 && kind == 0;
-  std::vector<std::pair<int, int>> snaps;  // (ring slot, snapshot index)
+  struct Snap {
+    int slot, si, iter;
+    bool fresh;
+  };
+  std::vector<Snap> snaps;
   int next_snap = 0;
-  auto take_snapshot = [&](int iter_no) {
+  auto enqueue_snapshot = [&](int iter_no) {
     if (!harvest || (int)snaps.size() >= 16 || iter_no != next_snap) return;
     next_snap = next_snap < 8 ? next_snap + 1 : next_snap * 2;
     // reservoir sampling over every pair offered so far (seeded, reproducible)
     int slot;
+    bool fresh = false;
     if (NT.count < NT.cap) {
       slot = NT.count++;
+      fresh = true;
     } else {
       NT.rs_state = NT.rs_state * 6364136223846793005ULL + 1442695040888963407ULL;
       const long long j = (long long)((NT.rs_state >> 11) % (uint64_t)(NT.offered + 1));
@@ -887,159 +920,135 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
     NT.offered++;
     if (slot < 0) return;
     const int si = (int)snaps.size();
-    k_d2f_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.r, NT.hr + (size_t)slot * N);
-    cudaMemcpyAsync(NT.xsnap + (size_t)si * N, x, N * 8, cudaMemcpyDeviceToDevice, st);
-    snaps.push_back({slot, si});
+    k_cg_snapshot<<<nb, 256, 0, st>>>(nw, c->lpoin_w, x, G.r, NT.xsnap + (size_t)si * N, NT.hr + (size_t)slot * N,
+                                      G.S);
+    snaps.push_back({slot, si, iter_no, fresh});
+  };
+  auto read_scalars = [&]() -> int {
+    CUDA_TRY(cudaMemcpyAsync(G.S_h, G.S, sizeof(CgScal), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(G.hist_h, G.hist, sizeof(double) * CG_HIST, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
+  };
+  // (re)start from the true FP64 residual: r = b - A x, z = M r, p = z
+  auto restart = [&]() -> int {
+    lap<double>(c, x, G.q);
+    k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
+    int rc2 = apply_precond(c, kind, G.r, G.z0);
+    if (rc2) return rc2;
+    dots<double, 2>(c, DotArgs<double, 2>{{G.r, G.r}, {G.z0, G.r}, {nullptr, nullptr}}, G.dots + 2);  // r.z, r.r
+    k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, G.z0, 0.0, G.p);
+    k_cg_start<<<1, 1, 0, st>>>(G.S, G.dots + 2, bnorm * bnorm * opts->tol * opts->tol, it);
+    return 0;
+  };
+  auto certify = [&]() -> int {
+    lap<double>(c, x, G.q);
+    k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
+    dots<double, 1>(c, DotArgs<double, 1>{{G.r}, {G.r}, {nullptr}}, G.dots + 2);
+    double h1;
+    CUDA_TRY(cudaMemcpyAsync(&h1, G.dots + 2, 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    res = std::sqrt(h1) / bnorm;
+    return 0;
+  };
+  // one iteration, entirely on the device: q = A p, alpha, x/r update,
+  // z = M r, beta, p = z + beta p
+  auto iteration = [&]() {
+    const MeshDev md = c->md();
+    dispatch(c, [&](auto L) {
+      using LL = decltype(L);
+      constexpr int P = LL::P_;
+      k_lap_elem<P, LL::EPB, double><<<LL::grid(c->nelem), LL::TPB, 0, st>>>(md, G.p, (double *)c->slotsB,
+                                                                             &G.S->status);
+      k_cg_q<<<cg_blocks(c->npoin, 2), CG_THREADS, 0, st>>>(md, (const double *)c->slotsB, G.p, G.q, G.S, G.gpart,
+                                                            G.ticket);
+      if (kind == 0) {
+        k_cg_update<true><<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.p, G.q, G.Minv, x, G.r, G.z0,
+                                                                     G.S, G.hist, CG_HIST, G.gpart, G.ticket);
+      } else {
+        using D = NetDims<P>;
+        k_cg_update<false><<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.p, G.q, G.Minv, x, G.r,
+                                                                      G.z0, G.S, G.hist, CG_HIST, G.gpart,
+                                                                      G.ticket, NT.Dh, NT.uf);
+        k_patch_apply_tc<P><<<2 * 148, 128, TcDims<P>::smem(), st>>>(c->nelem, NT.pt, NT.uf, NT.params, NT.gains,
+                                                                     c->slotsB, &G.S->status);
+        k_cg_patch_z<<<cg_blocks(c->npoin, 2), CG_THREADS, 0, st>>>(c->npoin, NT.pptr, NT.pslot, c->slotsB, G.r,
+                                                                    NT.Dh, NT.params, D::O_ALPHA, G.z0, G.S,
+                                                                    G.gpart, G.ticket);
+      }
+      k_cg_dir<<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.z0, G.p, G.S);
+      return 0;
+    });
   };
   if (bnorm == 0.0) {
     CUDA_TRY(cudaMemsetAsync(x, 0, N * 8, st));
-  } else if (kind == 0) {
+  } else {
     bool converged = false;
+    int breakdowns = 0;
     while (!converged && it < opts->max_iter) {
-      // (re)start: r = b - A x (FP64 true residual), z = M r, p = z
-      lap<double>(c, x, G.q);
-      k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
-      if ((rc = apply_precond(c, kind, G.r, G.z0))) return rc;
-      k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, G.z0, 0.0, G.p);
+      if ((rc = restart())) return rc;
+      if (it == 0) enqueue_snapshot(0);
       double best = 1e300;
-      int best_it = it;
-      take_snapshot(it);
-      for (; it < opts->max_iter;) {
-        ++it;
-        lap<double>(c, G.p, G.q);
-        dots<double, 2>(c, DotArgs<double, 2>{{G.r, G.p}, {G.z0, G.q}, {nullptr, nullptr}}, G.dots);
-        k_cg_update1<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.dots, x, G.r, G.p, G.q, G.z0, G.z1, G.Minv, 0, 0);
-        // z1 = z0 ; z0 = M r
-        CUDA_TRY(cudaMemcpyAsync(G.z1, G.z0, N * 8, cudaMemcpyDeviceToDevice, st));
-        if ((rc = apply_precond(c, kind, G.r, G.z0))) return rc;
-        dots<double, 2>(c, DotArgs<double, 2>{{G.r, G.r}, {G.r, G.z0}, {nullptr, G.z1}}, G.dots + 2);
-        double h[2];
-        CUDA_TRY(cudaMemcpyAsync(h, G.dots + 2, 16, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-        const double nrm = std::sqrt(h[0]) / bnorm;
-        if (!std::isfinite(nrm)) return fail(SOD_GPU_ENONFINITE, "non-finite residual in pressure solve");
-        if (nrm < best * 0.5) { best = nrm; best_it = it; }
-        if (nrm < opts->tol) {
-          // certify with the true FP64 residual
-          lap<double>(c, x, G.q);
-          k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
-          dots<double, 1>(c, DotArgs<double, 1>{{G.r}, {G.r}, {nullptr}}, G.dots + 2);
-          CUDA_TRY(cudaMemcpyAsync(h, G.dots + 2, 8, cudaMemcpyDeviceToHost, st));
-          CUDA_TRY(cudaStreamSynchronize(st));
-          res = std::sqrt(h[0]) / bnorm;
+      int best_it = it, batch = kind == 0 ? 16 : 8;
+      while (it < opts->max_iter) {
+        const int it0 = it, nbat = std::min(batch, opts->max_iter - it);
+        for (int k = 0; k < nbat; ++k) {
+          iteration();
+          enqueue_snapshot(it0 + k + 1);
+        }
+        if ((rc = read_scalars())) return rc;
+        const CgScal &S = *G.S_h;
+        it = S.iter;
+        if (S.status == 3) return fail(SOD_GPU_ENONFINITE, "non-finite residual in pressure solve");
+        if (S.status == 0 && it == it0) return fail(SOD_GPU_ESTAGNATE, "pressure solve made no progress");
+        // convergence history of this batch: stagnation check and next batch size
+        double first = -1.0, lastv = -1.0;
+        for (int k = it0; k < it; ++k) {
+          const double rr = G.hist_h[k % CG_HIST];
+          if (first < 0) first = rr;
+          lastv = rr;
+          const double nrm = std::sqrt(rr) / bnorm;
+          if (nrm < best * 0.5) { best = nrm; best_it = k + 1; }
+        }
+        if (lastv >= 0) res = std::sqrt(lastv) / bnorm;
+        if (S.status == 1) {
+          if ((rc = certify())) return rc;
           if (res < opts->tol) converged = true;
-          break;  // restart from the true residual if not yet certified
+          break;  // certified, or restart from the true residual
+        }
+        if (S.status == 2) {  // p.Ap <= 0 (loss of orthogonality): restart
+          if (++breakdowns > 3) return fail(SOD_GPU_ESTAGNATE, "repeated breakdown in pressure solve");
+          break;
         }
         if (kind != 0 && it - best_it > window) {  // stagnation: fall back to Jacobi
           kind = 0;
           fallback = 1;
           break;
         }
-        k_cg_update2<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.dots, G.dots + 2, G.p, G.z0);
-        res = nrm;
-        take_snapshot(it);
+        if (it - it0 >= 2 && first > 0 && lastv > 0 && lastv < first) {
+          const double rate = std::log(lastv / first) / (double)(it - it0 - 1);  // log rr per iteration
+          const double need = std::log(S.thr2 / lastv) / rate;
+          batch = (int)std::min(64.0, std::max(4.0, std::ceil(need) + 1.0));
+        }
       }
-    }
-  } else {
-    // truncated flexible CG with the learned preconditioner
-    const int m = opts->truncation > 0 ? (opts->truncation < 7 ? opts->truncation : 7) : 4;
-    if (!G.Pm && ((rc = c->alloc(&G.Pm, 7 * N)) || (rc = c->alloc(&G.Qm, 7 * N)))) return rc;
-    double pAp[7];
-    bool converged = false;
-    while (!converged && it < opts->max_iter) {
-      lap<double>(c, x, G.q);
-      k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
-      int nd = 0;  // stored directions
-      double best = 1e300;
-      int best_it = it;
-      bool restart = false;
-      while (!restart && it < opts->max_iter) {
-        if ((rc = apply_precond(c, kind, G.r, G.z0))) return rc;
-        // dots: ||r||^2 and z.Q_j for the stored directions (one pass)
-        const int nq = nd < m ? nd : m;
-        DotArgs<double, 8> A8{};
-        A8.a[0] = G.r; A8.b[0] = G.r; A8.c[0] = nullptr;
-        for (int j = 0; j < 7; ++j) {
-          A8.a[1 + j] = G.z0;
-          A8.b[1 + j] = (j < nq) ? G.Qm + (size_t)j * N : G.r;
-          A8.c[1 + j] = nullptr;
-        }
-        dots<double, 8>(c, A8, G.dots + 8);
-        double hd[8];
-        CUDA_TRY(cudaMemcpyAsync(hd, G.dots + 8, 64, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-        const double nrm = std::sqrt(hd[0]) / bnorm;
-        if (!std::isfinite(nrm)) return fail(SOD_GPU_ENONFINITE, "non-finite residual in pressure solve");
-        res = nrm;
-        if (nrm < best * 0.5) { best = nrm; best_it = it; }
-        if (nrm < opts->tol) {
-          lap<double>(c, x, G.q);
-          k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
-          dots<double, 1>(c, DotArgs<double, 1>{{G.r}, {G.r}, {nullptr}}, G.dots + 2);
-          double h1;
-          CUDA_TRY(cudaMemcpyAsync(&h1, G.dots + 2, 8, cudaMemcpyDeviceToHost, st));
-          CUDA_TRY(cudaStreamSynchronize(st));
-          res = std::sqrt(h1) / bnorm;
-          if (res < opts->tol) converged = true;
-          restart = true;
-          break;
-        }
-        if (it - best_it > window) {  // stagnation: fall back to Jacobi
-          kind = 0;
-          fallback = 1;
-          break;
-        }
-        // p = z - sum_j (z.Q_j / pAp_j) P_j   (A-orthogonal to the stored directions)
-        const int slot = nd % m;
-        MultiAxpy MA{};
-        MA.n = nq;
-        for (int j = 0; j < nq; ++j) {
-          MA.v[j] = G.Pm + (size_t)j * N;
-          MA.c[j] = -(hd[1 + j] / pAp[j]);
-        }
-        double *pnew = G.Pm + (size_t)slot * N, *qnew = G.Qm + (size_t)slot * N;
-        k_multi_axpy<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.z0, MA, G.p);
-        CUDA_TRY(cudaMemcpyAsync(pnew, G.p, N * 8, cudaMemcpyDeviceToDevice, st));
-        lap<double>(c, pnew, qnew);
-        dots<double, 2>(c, DotArgs<double, 2>{{pnew, pnew}, {qnew, G.r}, {nullptr, nullptr}}, G.dots + 2);
-        double ha[2];
-        CUDA_TRY(cudaMemcpyAsync(ha, G.dots + 2, 16, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaStreamSynchronize(st));
-        if (!(ha[0] > 0.0)) { restart = true; break; }  // lost positivity: restart from the true residual
-        pAp[slot] = ha[0];
-        const double alpha = ha[1] / ha[0];
-        k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, alpha, pnew, 1.0, x);
-        k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, -alpha, qnew, 1.0, G.r);
-        ++nd;
-        ++it;
-      }
-      if (kind == 0 && fallback) break;
-    }
-    if (fallback && !converged) {
-      // continue with Jacobi CG from the current iterate
-      sod_solve_opts_t o2 = *opts;
-      o2.precond = 0;
-      o2.harvest = 0;
-      o2.max_iter = opts->max_iter - it > 1 ? opts->max_iter - it : 1;
-      sod_solve_stats_t s2{};
-      int rc2 = sod_gpu_pressure_solve(c, b_in, x, &o2, &s2);
-      it += s2.iterations;
-      res = s2.res_rel;
-      if (rc2 && rc2 != SOD_GPU_ESTAGNATE) return rc2;
     }
   }
-  // harvested pairs: e_k = x* - x_k and their energy norms
+  // harvested pairs: keep snapshots taken before convergence; e_k = x* - x_k
   for (auto &sn : snaps) {
+    if (sn.iter >= it) {
+      if (sn.fresh) { NT.count--; NT.offered--; }
+      continue;
+    }
     double *e = NT.tmp1;
     k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, x, 0.0, e);
-    k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, -1.0, NT.xsnap + (size_t)sn.second * N, 1.0, e);
-    k_d2f_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, e, NT.he + (size_t)sn.first * N);
+    k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, -1.0, NT.xsnap + (size_t)sn.si * N, 1.0, e);
+    k_d2f_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, e, NT.he + (size_t)sn.slot * N);
     lap<double>(c, e, NT.tmp2);
     dots<double, 1>(c, DotArgs<double, 1>{{e}, {NT.tmp2}, {nullptr}}, G.dots + 5);
     double eAe = 0.0;
     CUDA_TRY(cudaMemcpyAsync(&eAe, G.dots + 5, 8, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    NT.eAe[sn.first] = eAe > 0 ? eAe : 1.0;
+    NT.eAe[sn.slot] = eAe > 0 ? eAe : 1.0;
   }
   CUDA_TRY(cudaEventRecord(e1, st));
   CUDA_TRY(cudaEventSynchronize(e1));
@@ -1070,6 +1079,26 @@ int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z) {
   }
   auto &NT = c->net;
   if (!NT.ready) return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
+  int rc;
+  if ((rc = ensure_gains(c))) return rc;
+  k_scale_f32<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, r, NT.Dh, NT.uf);
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    constexpr int P = LL::P_;
+    using D = NetDims<P>;
+    k_patch_apply_tc<P><<<2 * 148, 128, TcDims<P>::smem(), c->stream>>>(c->nelem, NT.pt, NT.uf, NT.params,
+                                                                        NT.gains, c->slotsB, nullptr);
+    k_patch_gather<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, NT.pptr, NT.pslot, c->slotsB, r, NT.Dh,
+                                                               NT.params, D::O_ALPHA, z);
+    return 0;
+  });
+  return 0;
+}
+
+// FP32 (CUDA-core) forward of the same map, used by training so that the
+// gradients follow the FP32 parameters exactly.
+int net_forward_fp32(sod_gpu_ctx *c, const double *r, double *z) {
+  auto &NT = c->net;
   int rc;
   if ((rc = ensure_gains(c))) return rc;
   dispatch(c, [&](auto L) {
@@ -1472,7 +1501,7 @@ int net_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double eAe, 
   const int nw = c->npoin_w;
   const unsigned nb = nblk(nw, 256);
   int rc;
-  if ((rc = ensure_train_scratch(c)) || (rc = apply_precond(c, 1, r, NT.tmp1))) return rc;  // z
+  if ((rc = ensure_train_scratch(c)) || (rc = net_forward_fp32(c, r, NT.tmp1))) return rc;  // z
   k_axpby<double><<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, 1.0, e, -1.0, NT.tmp1);        // d = e - z
   lap<double>(c, NT.tmp1, NT.tmp2);                                                         // A d
   dots<double, 1>(c, DotArgs<double, 1>{{NT.tmp1}, {NT.tmp2}, {nullptr}}, G.dots + 2);
@@ -1598,7 +1627,8 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
         (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.pt, NPt)) ||
         (rc = c->alloc(&NT.pptr, (size_t)c->npoin + 1)) || (rc = c->alloc(&NT.pslot, NPt)) ||
         (rc = c->alloc(&NT.feat, (size_t)E * NET_F)) || (rc = c->alloc(&NT.gains, (size_t)E * NET_K)) ||
-        (rc = c->alloc(&NT.Dh, (size_t)c->npoin)) || (rc = c->alloc(&NT.tmp1, (size_t)c->npoin)) ||
+        (rc = c->alloc(&NT.Dh, (size_t)c->npoin)) || (rc = c->alloc(&NT.uf, (size_t)c->npoin)) ||
+        (rc = c->alloc(&NT.tmp1, (size_t)c->npoin)) ||
         (rc = c->alloc(&NT.tmp2, (size_t)c->npoin)))
       return rc;
     if (P == 3) {
@@ -1606,11 +1636,15 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
       CUDA_TRY(cudaFuncSetAttribute(k_mlp_bwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * D::NMLP * 4));
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_apply_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TcDims<3>::smem()));
     } else {
       using D = NetDims<4>;
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
       CUDA_TRY(cudaFuncSetAttribute(k_mlp_bwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * D::NMLP * 4));
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_apply_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)TcDims<4>::smem()));
     }
     // patch table and its node-centric CSR (slots in increasing (e, j) order)
     std::vector<int> conn((size_t)E * N), pt;

@@ -29,7 +29,7 @@ class SodMesh(C.Structure):
 
 class SolveOpts(C.Structure):
     _fields_ = [("max_iter", C.c_int), ("tol", C.c_double), ("precond", C.c_int), ("stagnation_window", C.c_int),
-                ("harvest", C.c_int), ("truncation", C.c_int)]
+                ("harvest", C.c_int)]
 
 
 class SolveStats(C.Structure):

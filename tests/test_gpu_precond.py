@@ -52,14 +52,14 @@ def test_loss_and_gradient_match_oracle(gpu, porder):
     e[w] = rng.normal(size=w.size)
     r = O.laplacian(om, e)
     dr, de = torch.from_numpy(r).cuda(), torch.from_numpy(e).cuda()
-    # inference
+    # inference (tensor cores, TF32 operands with FP32 accumulation: ~1e-3)
     z = torch.zeros(m.npoin, dtype=torch.float64, device="cuda")
     ctx.call("sod_gpu_precond_apply", gpu.dptr(dr), gpu.dptr(z))
     zr, _ = net.forward(params.astype(np.float64), r)
     zerr = np.linalg.norm(z.cpu().numpy()[w] - zr[w]) / np.linalg.norm(zr[w])
     print("apply rel L2", zerr)
-    assert zerr < 1e-5
-    # loss and gradient
+    assert zerr < 3e-3
+    # loss and gradient (FP32 forward and backward kernels)
     ref_loss, ref_grad = net.loss_grad(params.astype(np.float64), r, e, lambda v: O.laplacian(om, v))
     loss = C.c_double()
     grad = np.zeros(n, np.float32)
