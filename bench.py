@@ -170,7 +170,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_steps=600):
+def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_steps=300, lr=1e-3):
     """Pressure-Poisson solve to a 1e-8 FP64-certified relative residual on
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG against the learned
@@ -199,7 +199,7 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
     loss = C.c_float()
     t0 = time.perf_counter()
-    ctxs[0].call("sod_gpu_precond_train", train_steps, 16, 3e-3, 7, C.byref(loss))
+    ctxs[0].call("sod_gpu_precond_train", train_steps, 16, lr, 7, C.byref(loss))
     train_s = time.perf_counter() - t0
     res = {}
     for i, (name, kind) in enumerate((("jacobi", 0), ("learned", 1))):
@@ -218,7 +218,7 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
         c.close()
     return {"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
                         f"projection-step pressure systems, FP64-certified tol 1e-8",
-            "harvest_steps": harvest_steps, "train_steps": train_steps, "train_seconds": round(train_s, 2),
+            "harvest_steps": harvest_steps, "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
             "final_training_loss": round(float(loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],
             "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3)}
 
@@ -241,14 +241,28 @@ def main():
     ap.add_argument("--nelem1d", type=int, default=NELEM_1D)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pressure", action="store_true")
+    ap.add_argument("--pressure-only", action="store_true",
+                    help="run only the pressure-solve comparison (prints its JSON object)")
+    ap.add_argument("--p-nelem1d", type=int, default=32)
+    ap.add_argument("--p-harvest", type=int, default=40)
+    ap.add_argument("--p-compare", type=int, default=20)
+    ap.add_argument("--p-train", type=int, default=300)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    pkw = dict(nelem1d=args.p_nelem1d, harvest_steps=args.p_harvest, compare_steps=args.p_compare,
+               train_steps=args.p_train)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.pressure_only:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps({"pressure_solve": pressure_leg(**pkw)}))
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -352,7 +366,7 @@ def main():
     }
     ctx.close()
     if rank == 0 and world == 1 and not args.no_pressure:
-        line["pressure_solve"] = pressure_leg()
+        line["pressure_solve"] = pressure_leg(**pkw)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = CpuBaseline().sample()
     if rank == 0:

@@ -114,6 +114,16 @@ int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *ctx, float Cp, float Pr, const float
                                const float *ProjMY, const float *ProjMZ, const float *tau_stab,
                                float *Rmass, float *Rmom, float *Rener, int initialze, float fact);
 
+/* Plain (not LPS-stabilised) diffusion residual; replaces
+ * full_diffusion_ijk, src/lib_sod2d/sources/elem_diffu.f90:12-223 (the
+ * path of flag_lps_stab = .false.).  Same argument meaning as
+ * sod_gpu_full_diff_stab_ijk without the projections and tau_stab;
+ * mu_e, mu_sgs are (nelem,ngaus); mu_sgs may be NULL (zero). */
+int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *ctx, float Cp, float Pr, const float *rho_n, const float *rho,
+                               const float *u, const float *Tem, const float *mu_fluid, const float *mu_e,
+                               const float *mu_sgs, float *Rmass, float *Rmom, float *Rener, int initialze,
+                               float fact);
+
 /* R(lpoin_w,:) *= invMl for ncomp components of an (npoin,ncomp) array.
  * Replaces lumped_solver_scal_opt / lumped_solver_vect_opt,
  * src/lib_sod2d/sources/mod_solver.f90:41-104. */

@@ -445,15 +445,15 @@ k_cg_update(int npoin_w, const int *__restrict__ lpoin_w, const double *__restri
 }
 
 // Learned preconditioner: z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of
-// the node's patch slots) (as k_patch_gather), with the partials r.z and
-// r.z_old; the last block sets beta and rz.
+// the node's contributions, stored contiguously from pptr[n]) (as
+// k_patch_gather_perm), with the partials r.z and r.z_old; the last block
+// sets beta and rz.
 __global__ void __launch_bounds__(CG_THREADS)
-k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const int *__restrict__ pslot,
-             const float *__restrict__ slots, const double *__restrict__ r, const double *__restrict__ Dh,
-             const float *__restrict__ prm, int o_alpha, double *__restrict__ z, CgScal *S,
-             double *__restrict__ part, unsigned *ticket) {
+k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const float *__restrict__ ctr,
+             const double *__restrict__ r, const double *__restrict__ Dh, const float *__restrict__ prm, int o_alpha,
+             double *__restrict__ z, CgScal *S, double *__restrict__ part, unsigned *ticket) {
   if (S->status) return;
-  constexpr int U = 2, MS = 8;
+  constexpr int U = CG_U;
   const double gam = exp((double)prm[o_alpha]);
   double v[2] = {0.0, 0.0};
   for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < npoin;
@@ -474,15 +474,12 @@ k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const int *__restric
       if (b[u] == en[u]) continue;
       const long long n = base + (long long)u * blockDim.x;
       double acc = 0.0;
-      for (int s0 = b[u]; s0 < en[u]; s0 += MS) {
-        int id[MS];
-        float y[MS];
+      for (int s0 = b[u]; s0 < en[u]; s0 += 8) {
+        float y[8];
 #pragma unroll
-        for (int k = 0; k < MS; ++k) id[k] = s0 + k < en[u] ? pslot[s0 + k] : -1;
+        for (int k = 0; k < 8; ++k) y[k] = s0 + k < en[u] ? ctr[s0 + k] : 0.f;
 #pragma unroll
-        for (int k = 0; k < MS; ++k) y[k] = id[k] >= 0 ? slots[id[k]] : 0.f;
-#pragma unroll
-        for (int k = 0; k < MS; ++k) acc += (double)y[k];
+        for (int k = 0; k < 8; ++k) acc += (double)y[k];
       }
       const double zn = dv[u] * (gam * dv[u] * rv[u] + acc);
       z[n] = zn;

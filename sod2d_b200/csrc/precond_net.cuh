@@ -226,10 +226,11 @@ struct TcDims {
   static constexpr int KP = (D::NP + 7) / 8 * 8;                   // slots padded to the mma k/n step
   static constexpr int S1 = KP + 4;                                // B as [mode][slot]: stride = 4 mod 8
   static constexpr int S2 = KP + ((8 - KP % 16) + 16) % 16;        // B as [mode][slot]: stride = 8 or 24 mod 32
-  static constexpr int SX = KP + 4;                                // X tile [16][SX]
   static constexpr int SY = NET_K + 4;                             // Y tile [16][SY]
-  static constexpr int WARPS = 4;
-  static constexpr size_t smem() { return (size_t)(NET_K * S1 + NET_K * S2 + WARPS * 16 * (SX + SY)) * 4; }
+  static constexpr int WARPS = 8;
+  static constexpr int KC = 10;                                    // k-steps whose operands are gathered together
+  static constexpr int NC = 10;                                    // output n-tiles whose positions are loaded together
+  static constexpr size_t smem() { return (size_t)(NET_K * S1 + NET_K * S2 + WARPS * 16 * SY) * 4; }
 };
 
 __device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
@@ -250,19 +251,24 @@ __global__ void k_scale_f32(int npoin_w, const int *__restrict__ lpoin_w, const 
   uf[i] = (float)(Dh[i] * r[i]);
 }
 
+// Each lane gathers exactly the A-fragment entries it needs (rows g, g+8 of
+// the 16 patches, columns t, t+4 of each k-step) straight from the patch
+// table, so no X tile is staged; outputs go to their node-ordered positions
+// pos[e][j] so that the assembly reads each node's contributions
+// contiguously.
 template <int P>
-__global__ void __launch_bounds__(128)
-k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const float *__restrict__ uf,
-                 const float *__restrict__ prm, const float *__restrict__ gains, float *__restrict__ slots,
-                 const int *__restrict__ stop) {
+__global__ void __launch_bounds__(256)
+k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restrict__ pos,
+                 const float *__restrict__ uf, const float *__restrict__ prm, const float *__restrict__ gains,
+                 float *__restrict__ out, const int *__restrict__ stop) {
   using D = NetDims<P>;
   using T = TcDims<P>;
-  constexpr int NP = D::NP, KP = T::KP, K = NET_K, JN = (KP + 31) / 32, NT2 = KP / 8;
+  constexpr int NP = D::NP, KP = T::KP, K = NET_K, NT2 = KP / 8, KS = KP / 8, KC = T::KC;
   if (stop && *stop) return;
   extern __shared__ __align__(16) float smem[];
   float *B1 = smem, *B2 = B1 + K * T::S1;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  float *X = B2 + K * T::S2 + warp * 16 * (T::SX + T::SY), *Y = X + 16 * T::SX;
+  float *Y = B2 + K * T::S2 + warp * 16 * T::SY;
   for (int i = threadIdx.x; i < K * KP; i += blockDim.x) {
     const int k = i / KP, j = i % KP;
     const float b = j < NP ? prm[D::O_B + k * NP + j] : 0.f;
@@ -274,59 +280,51 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const float *__res
   const long long ngroups = (nelem + 15) / 16;
   for (long long grp = (long long)blockIdx.x * T::WARPS + warp; grp < ngroups;
        grp += (long long)gridDim.x * T::WARPS) {
-    const long long e0 = grp * 16;
-    // gather X = D^-1/2 r over the 16 patches (indices first, then values)
-#pragma unroll 1
-    for (int r0 = 0; r0 < 16; r0 += 4) {
-      int id[4][JN];
-#pragma unroll
-      for (int rr = 0; rr < 4; ++rr)
-#pragma unroll
-        for (int q = 0; q < JN; ++q) {
-          const long long e = e0 + r0 + rr;
-          const int j = lane + 32 * q;
-          id[rr][q] = (e < nelem && j < NP) ? pt[e * NP + j] : -1;
-        }
-      float xv[4][JN];
-#pragma unroll
-      for (int rr = 0; rr < 4; ++rr)
-#pragma unroll
-        for (int q = 0; q < JN; ++q) xv[rr][q] = id[rr][q] >= 0 ? uf[id[rr][q]] : 0.f;
-#pragma unroll
-      for (int rr = 0; rr < 4; ++rr)
-#pragma unroll
-        for (int q = 0; q < JN; ++q) {
-          const int j = lane + 32 * q;
-          if (j < KP) X[(r0 + rr) * T::SX + j] = xv[rr][q];
-        }
-    }
-    __syncwarp();
-    // H = X B^T : 4 n-tiles of 8 modes, KP/8 k-steps
+    const long long ea = grp * 16 + g, eb = ea + 8;
+    const bool va = ea < nelem, vb = eb < nelem;
+    const int *pa = pt + ea * NP, *pb = pt + eb * NP;
+    // H = X B^T : 4 n-tiles of 8 modes, KS k-steps gathered KC at a time
     float h[4][4];
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q) h[nt][q] = 0.f;
-#pragma unroll 4
-    for (int k0 = 0; k0 < KP; k0 += 8) {
-      const uint32_t a0 = __float_as_uint(X[g * T::SX + k0 + t]);
-      const uint32_t a1 = __float_as_uint(X[(g + 8) * T::SX + k0 + t]);
-      const uint32_t a2 = __float_as_uint(X[g * T::SX + k0 + t + 4]);
-      const uint32_t a3 = __float_as_uint(X[(g + 8) * T::SX + k0 + t + 4]);
+#pragma unroll 1
+    for (int c0 = 0; c0 < KS; c0 += KC) {
+      int id[KC][4];
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const uint32_t b0 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t]);
-        const uint32_t b1 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t + 4]);
-        mma_tf32(h[nt], a0, a1, a2, a3, b0, b1);
+      for (int kk = 0; kk < KC; ++kk) {
+        const int k0 = (c0 + kk) * 8, ca = k0 + t, cb = k0 + t + 4;
+        const bool in = c0 + kk < KS;
+        id[kk][0] = (in && va && ca < NP) ? pa[ca] : -1;
+        id[kk][1] = (in && vb && ca < NP) ? pb[ca] : -1;
+        id[kk][2] = (in && va && cb < NP) ? pa[cb] : -1;
+        id[kk][3] = (in && vb && cb < NP) ? pb[cb] : -1;
+      }
+      float xv[KC][4];
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) xv[kk][q] = id[kk][q] >= 0 ? uf[id[kk][q]] : 0.f;
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk) {
+        if (c0 + kk >= KS) break;
+        const int k0 = (c0 + kk) * 8;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const uint32_t b0 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t]);
+          const uint32_t b1 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t + 4]);
+          mma_tf32(h[nt], __float_as_uint(xv[kk][0]), __float_as_uint(xv[kk][1]), __float_as_uint(xv[kk][2]),
+                   __float_as_uint(xv[kk][3]), b0, b1);
+        }
       }
     }
-    // Y = gains * H
+    // Y = gains * H (through shared memory into the A-fragment layout)
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
       const int col = nt * 8 + 2 * t;
-      const long long ea = e0 + g, eb = e0 + g + 8;
-      const float2 sa = ea < nelem ? *reinterpret_cast<const float2 *>(gains + ea * K + col) : make_float2(0.f, 0.f);
-      const float2 sb = eb < nelem ? *reinterpret_cast<const float2 *>(gains + eb * K + col) : make_float2(0.f, 0.f);
+      const float2 sa = va ? *reinterpret_cast<const float2 *>(gains + ea * K + col) : make_float2(0.f, 0.f);
+      const float2 sb = vb ? *reinterpret_cast<const float2 *>(gains + eb * K + col) : make_float2(0.f, 0.f);
       Y[g * T::SY + col] = sa.x * h[nt][0];
       Y[g * T::SY + col + 1] = sa.y * h[nt][1];
       Y[(g + 8) * T::SY + col] = sb.x * h[nt][2];
@@ -342,30 +340,55 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const float *__res
       a[kk][2] = __float_as_uint(Y[g * T::SY + k0 + t + 4]);
       a[kk][3] = __float_as_uint(Y[(g + 8) * T::SY + k0 + t + 4]);
     }
-    // O = Y B : KP/8 n-tiles of 8 slots, 4 k-steps
-#pragma unroll 2
-    for (int nt = 0; nt < NT2; ++nt) {
-      float o[4] = {0.f, 0.f, 0.f, 0.f};
+    __syncwarp();
+    // O = Y B : KP/8 n-tiles of 8 slots, 4 k-steps; scattered to pos, whose
+    // entries are loaded NC n-tiles at a time
+    const int *qa = pos + ea * NP, *qb = pos + eb * NP;
+#pragma unroll 1
+    for (int n0 = 0; n0 < NT2; n0 += T::NC) {
+      int w[T::NC][4];
 #pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const int k0 = kk * 8;
-        const uint32_t b0 = __float_as_uint(B2[(k0 + t) * T::S2 + nt * 8 + g]);
-        const uint32_t b1 = __float_as_uint(B2[(k0 + t + 4) * T::S2 + nt * 8 + g]);
-        mma_tf32(o, a[kk][0], a[kk][1], a[kk][2], a[kk][3], b0, b1);
+      for (int nn = 0; nn < T::NC; ++nn) {
+        const int col = (n0 + nn) * 8 + 2 * t;
+        const bool in = n0 + nn < NT2;
+        w[nn][0] = (in && va && col < NP) ? qa[col] : -1;
+        w[nn][1] = (in && va && col + 1 < NP) ? qa[col + 1] : -1;
+        w[nn][2] = (in && vb && col < NP) ? qb[col] : -1;
+        w[nn][3] = (in && vb && col + 1 < NP) ? qb[col + 1] : -1;
       }
-      const int col = nt * 8 + 2 * t;
-      const long long ea = e0 + g, eb = e0 + g + 8;
-      if (ea < nelem) {
-        if (col < NP) slots[ea * NP + col] = o[0];
-        if (col + 1 < NP) slots[ea * NP + col + 1] = o[1];
-      }
-      if (eb < nelem) {
-        if (col < NP) slots[eb * NP + col] = o[2];
-        if (col + 1 < NP) slots[eb * NP + col + 1] = o[3];
+#pragma unroll
+      for (int nn = 0; nn < T::NC; ++nn) {
+        if (n0 + nn >= NT2) break;
+        const int nt = n0 + nn;
+        float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const int k0 = kk * 8;
+          const uint32_t b0 = __float_as_uint(B2[(k0 + t) * T::S2 + nt * 8 + g]);
+          const uint32_t b1 = __float_as_uint(B2[(k0 + t + 4) * T::S2 + nt * 8 + g]);
+          mma_tf32(o, a[kk][0], a[kk][1], a[kk][2], a[kk][3], b0, b1);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if (w[nn][q] >= 0) out[w[nn][q]] = o[q];
       }
     }
-    __syncwarp();
   }
+}
+
+// z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of the node's
+// contributions, stored contiguously from pptr[n]), FP64.
+__global__ void k_patch_gather_perm(long long npoin, const int *__restrict__ pptr, const float *__restrict__ ctr,
+                                    const double *__restrict__ r, const double *__restrict__ Dh,
+                                    const float *__restrict__ prm, int o_alpha, double *__restrict__ z) {
+  const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= npoin) return;
+  const int b = pptr[n], en = pptr[n + 1];
+  if (b == en) return;
+  double acc = 0.0;
+  for (int s = b; s < en; ++s) acc += (double)ctr[s];
+  const double d = Dh[n];
+  z[n] = d * (exp((double)prm[o_alpha]) * d * r[n] + acc);
 }
 
 // z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of the node's patch

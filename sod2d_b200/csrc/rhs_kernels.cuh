@@ -188,13 +188,15 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
 // of width 8: {mass, energy, mom x, mom y, mom z, 0, 0, 0}.
 //
 // MODE_CONV: convective residual * fact_c.
-// MODE_DIFF: LPS-stabilised diffusion * fact_d.
+// MODE_DIFF: LPS-stabilised diffusion * fact_d (full_diff_stab_ijk);
+//   with MODE_NOLPS the plain diffusion of full_diffusion_ijk
+//   (elem_diffu.f90:12-223).
 // Input kinds:
 //   IN_CONS : a0 = rho, a1 = q(N,3), a2 = E (conserved; EOS fused, h = E:=aux_h)
 //   IN_PRIM : convection inputs u, q, rho, pr, E given directly
 //   IN_DIFF : diffusion inputs rho, u, Tem, mu_fluid given directly
 // ---------------------------------------------------------------------
-enum { MODE_CONV = 1, MODE_DIFF = 2 };
+enum { MODE_CONV = 1, MODE_DIFF = 2, MODE_NOLPS = 4 };
 enum { IN_CONS = 0, IN_PRIM = 1, IN_DIFF = 2 };
 
 struct RhsArgs {
@@ -376,10 +378,14 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   }
 
   if (DIFF) {
+    constexpr bool LPS = (MODE & MODE_NOLPS) == 0;
+    constexpr int NC = LPS ? 5 : 6;  // staged contravariant flux fields
     // Fluxes at this Gauss point (first Gauss-point loop of
-    // full_diff_stab_ijk, elem_stab.f90:296-385), then their contravariant
-    // components gpvol * sum_i He(i,d) F_i, staged for the weak divergence.
-    float C[5][3];
+    // full_diff_stab_ijk, elem_stab.f90:296-385, or of full_diffusion_ijk,
+    // elem_diffu.f90:99-164), then their contravariant components
+    // gpvol * sum_i He(i,d) F_i, staged for the weak divergence.
+    float C[NC][3];
+    float nu_e = 0.f, kappa_e = 0.f;
     if (active) {
       float(*f)[N] = sm[el];
       float a0, a1, a2, gradT[3];
@@ -389,34 +395,35 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
       const float mue = A.mue_t[e * N + t];
       const float musgs = A.musgs_t ? A.musgs_t[e * N + t] : 0.f;
       const float rhon = s.rho;
-      const float nu_e = ph.c_rho * mue / rhon;
+      nu_e = ph.c_rho * mue / rhon;
       const float mu_fgp = mu + rhon * musgs;
       const float mu_egp = mue;
-      const float kappa_e = mu * ph.Cp / ph.Prt + ph.c_ener * mue * ph.Cp / ph.Prt +
-                            ph.Cp * rhon * musgs / 0.9f;
-      const float ts = A.tau_stab[e];
+      kappa_e = mu * ph.Cp / ph.Prt + ph.c_ener * mue * ph.Cp / ph.Prt + ph.Cp * rhon * musgs / 0.9f;
       const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
-      float tau[3][3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-#pragma unroll
-        for (int b = 0; b < 3; ++b) tau[a][b] = gradU[a][b] + gradU[b][a];
-        tau[a][a] = tau[a][a] - ph.twoThirds * divU;
-      }
-      const float4 *pj = reinterpret_cast<const float4 *>(A.proj12 + (long long)node * 12);
-      const float4 p0 = pj[0], p1 = pj[1], p2 = pj[2];
-      const float PX[3] = {p0.x, p0.y, p0.z}, PY[3] = {p0.y, p0.w, p1.x}, PZ[3] = {p0.z, p1.x, p1.y};
-      const float PM[3] = {p1.z, p1.w, p2.x}, PE[3] = {p2.y, p2.z, p2.w};
       const float u[3] = {s.u0, s.u1, s.u2};
+      float tau[3][3];
       float Fx[3], Fy[3], Fz[3], FT[3], FR[3];
-      const float cl = -ph.c_lps * ts;
+      if (LPS) {
+        const float ts = A.tau_stab[e];
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        Fx[d] = cl * (PX[d] - tau[0][d]) * rhon;
-        Fy[d] = cl * (PY[d] - tau[1][d]) * rhon;
-        Fz[d] = cl * (PZ[d] - tau[2][d]) * rhon;
-        FT[d] = cl * (PE[d] - gradT[d]) * rhon * ph.Cp / ph.Prt;
-        FR[d] = cl * (PM[d] - gradRho[d]);
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+          for (int b = 0; b < 3; ++b) tau[a][b] = gradU[a][b] + gradU[b][a];
+          tau[a][a] = tau[a][a] - ph.twoThirds * divU;
+        }
+        const float4 *pj = reinterpret_cast<const float4 *>(A.proj12 + (long long)node * 12);
+        const float4 p0 = pj[0], p1 = pj[1], p2 = pj[2];
+        const float PX[3] = {p0.x, p0.y, p0.z}, PY[3] = {p0.y, p0.w, p1.x}, PZ[3] = {p0.z, p1.x, p1.y};
+        const float PM[3] = {p1.z, p1.w, p2.x}, PE[3] = {p2.y, p2.z, p2.w};
+        const float cl = -ph.c_lps * ts;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          Fx[d] = cl * (PX[d] - tau[0][d]) * rhon;
+          Fy[d] = cl * (PY[d] - tau[1][d]) * rhon;
+          Fz[d] = cl * (PZ[d] - tau[2][d]) * rhon;
+          FT[d] = cl * (PE[d] - gradT[d]) * rhon * ph.Cp / ph.Prt;
+          FR[d] = cl * (PM[d] - gradRho[d]);
+        }
       }
       float tauU[3] = {0.f, 0.f, 0.f};
       const float mt = mu_fgp + mu_egp;
@@ -430,13 +437,26 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
         tauU[a] = tauU[a] - (mu_fgp)*ph.twoThirds * divU * u[a];
         tau[a][a] = tau[a][a] - (mu_fgp)*ph.twoThirds * divU;
       }
+      if (LPS) {
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        Fx[d] = Fx[d] + tau[0][d];
-        Fy[d] = Fy[d] + tau[1][d];
-        Fz[d] = Fz[d] + tau[2][d];
-        FT[d] = FT[d] + kappa_e * gradT[d] + tauU[d];
-        FR[d] = FR[d] + nu_e * gradRho[d];
+        for (int d = 0; d < 3; ++d) {
+          Fx[d] = Fx[d] + tau[0][d];
+          Fy[d] = Fy[d] + tau[1][d];
+          Fz[d] = Fz[d] + tau[2][d];
+          FT[d] = FT[d] + kappa_e * gradT[d] + tauU[d];
+          FR[d] = FR[d] + nu_e * gradRho[d];
+        }
+      } else {
+        // full_diffusion_ijk scales the neighbours' grad rho and grad T by
+        // nu_e and kappa_e of the output Gauss point: stage them unscaled.
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          Fx[d] = tau[0][d];
+          Fy[d] = tau[1][d];
+          Fz[d] = tau[2][d];
+          FT[d] = tauU[d];
+          FR[d] = gradRho[d];
+        }
       }
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
@@ -446,12 +466,13 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
         C[2][d] = gv * (h0 * Fx[0] + h1 * Fx[1] + h2 * Fx[2]);
         C[3][d] = gv * (h0 * Fy[0] + h1 * Fy[1] + h2 * Fy[2]);
         C[4][d] = gv * (h0 * Fz[0] + h1 * Fz[1] + h2 * Fz[2]);
+        if (!LPS) C[NC - 1][d] = gv * (h0 * gradT[0] + h1 * gradT[1] + h2 * gradT[2]);
       }
     }
     __syncthreads();  // all reads of the staged fields are done
     if (active) {
 #pragma unroll
-      for (int q = 0; q < 5; ++q)
+      for (int q = 0; q < NC; ++q)
 #pragma unroll
         for (int d = 0; d < 3; ++d) sm[el][q * 3 + d][t] = C[q][d];
     }
@@ -461,8 +482,9 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
       float Dci[N1], Dcj[N1], Dck[N1];
 #pragma unroll
       for (int q = 0; q < N1; ++q) { Dci[q] = m.Dnat[q * N1 + i]; Dcj[q] = m.Dnat[q * N1 + j]; Dck[q] = m.Dnat[q * N1 + k]; }
+      float wd[NC];
 #pragma unroll
-      for (int q = 0; q < 5; ++q) {
+      for (int q = 0; q < NC; ++q) {
         const float *c0 = sm[el][q * 3 + 0], *c1 = sm[el][q * 3 + 1], *c2 = sm[el][q * 3 + 2];
         float acc = 0.f;
 #pragma unroll
@@ -472,14 +494,23 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
           acc = fmaf(Dcj[mm], c1[i + N1 * mm + N1 * N1 * k], acc);
           acc = fmaf(Dck[mm], c2[i + N1 * j + N1 * N1 * mm], acc);
         }
-        res[q] = res[q] + A.fact_d * acc;
+        wd[q] = acc;
+      }
+      if (LPS) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) res[q] = res[q] + A.fact_d * wd[q];
+      } else {
+        res[0] = res[0] + A.fact_d * (nu_e * wd[0]);
+        res[1] = res[1] + A.fact_d * (wd[1] + kappa_e * wd[NC - 1]);
+#pragma unroll
+        for (int q = 2; q < 5; ++q) res[q] = res[q] + A.fact_d * wd[q];
       }
     }
   }
   if (active) {
-    float4 *o = reinterpret_cast<float4 *>(slots + (e * N + t) * 8);
-    o[0] = make_float4(res[0], res[1], res[2], res[3]);
-    o[1] = make_float4(res[4], 0.f, 0.f, 0.f);
+    // pass-B slots: [E*N] float4 (mass, energy, mom x, mom y), then [E*N] mom z
+    reinterpret_cast<float4 *>(slots)[e * N + t] = make_float4(res[0], res[1], res[2], res[3]);
+    slots[(long long)m.nelem * N * 4 + e * N + t] = res[4];
   }
 }
 
@@ -499,6 +530,7 @@ __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__re
                          OutPtrs out_soa, int accumulate, int use_invMl) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= m.npoin) return;
+  constexpr int MS = W >= 12 ? 1 : 4;  // slots whose loads are issued together (registers permitting)
   float sum[NFO], cmp[NFO];
 #pragma unroll
   for (int f = 0; f < NFO; ++f) {
@@ -506,20 +538,32 @@ __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__re
     cmp[f] = 0.f;
   }
   const int b = m.slot_ptr[p], en = m.slot_ptr[p + 1];
-  for (int s = b; s < en; ++s) {
-    const float4 *v = reinterpret_cast<const float4 *>(slots + (long long)m.slot_idx[s] * W);
-    float x[W];
+  for (int s0 = b; s0 < en; s0 += MS) {
+    int id[MS];
 #pragma unroll
-    for (int c = 0; c < W / 4; ++c) {
-      float4 t4 = v[c];
-      x[4 * c] = t4.x; x[4 * c + 1] = t4.y; x[4 * c + 2] = t4.z; x[4 * c + 3] = t4.w;
-    }
+    for (int k = 0; k < MS; ++k) id[k] = s0 + k < en ? m.slot_idx[s0 + k] : -1;
+    float4 v[MS][W / 4];
 #pragma unroll
-    for (int f = 0; f < NFO; ++f) {  // Kahan summation
-      const float y = x[f] - cmp[f];
-      const float tt = sum[f] + y;
-      cmp[f] = (tt - sum[f]) - y;
-      sum[f] = tt;
+    for (int k = 0; k < MS; ++k)
+#pragma unroll
+      for (int c = 0; c < W / 4; ++c)
+        v[k][c] = id[k] >= 0 ? reinterpret_cast<const float4 *>(slots + (long long)id[k] * W)[c]
+                             : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < MS; ++k) {
+      if (id[k] < 0) break;
+      float x[W];
+#pragma unroll
+      for (int c = 0; c < W / 4; ++c) {
+        x[4 * c] = v[k][c].x; x[4 * c + 1] = v[k][c].y; x[4 * c + 2] = v[k][c].z; x[4 * c + 3] = v[k][c].w;
+      }
+#pragma unroll
+      for (int f = 0; f < NFO; ++f) {  // Kahan summation
+        const float y = x[f] - cmp[f];
+        const float tt = sum[f] + y;
+        cmp[f] = (tt - sum[f]) - y;
+        sum[f] = tt;
+      }
     }
   }
   const float sc = use_invMl ? m.invMl[p] : 1.f;
@@ -534,6 +578,53 @@ __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__re
 #pragma unroll
     for (int f = 0; f < NFO; ++f) out_soa.p[f][p] = sum[f] * sc;
   }
+}
+
+// Assembly of the pass-B slots of k_rhs ([E*N] float4 of mass, energy,
+// mom x, mom y, then [E*N] floats of mom z) into the 5 SoA residuals, same
+// summation order and Kahan compensation as k_gather.
+// zoff = nelem * nodes per element (start of the mom-z block, in floats / 4).
+__global__ void k_gather_res5(MeshDev m, const float *__restrict__ slots, long long zoff, OutPtrs out_soa,
+                              int accumulate, int use_invMl) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= m.npoin) return;
+  constexpr int MS = 4;
+  const float *sz = slots + 4 * zoff;
+  float sum[5], cmp[5];
+#pragma unroll
+  for (int f = 0; f < 5; ++f) {
+    sum[f] = accumulate ? out_soa.p[f][p] : 0.f;
+    cmp[f] = 0.f;
+  }
+  const int b = m.slot_ptr[p], en = m.slot_ptr[p + 1];
+  const float4 *s4 = reinterpret_cast<const float4 *>(slots);
+  for (int s0 = b; s0 < en; s0 += MS) {
+    int id[MS];
+#pragma unroll
+    for (int k = 0; k < MS; ++k) id[k] = s0 + k < en ? m.slot_idx[s0 + k] : -1;
+    float4 v[MS];
+    float w[MS];
+#pragma unroll
+    for (int k = 0; k < MS; ++k) {
+      v[k] = id[k] >= 0 ? s4[id[k]] : make_float4(0.f, 0.f, 0.f, 0.f);
+      w[k] = id[k] >= 0 ? sz[id[k]] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < MS; ++k) {
+      if (id[k] < 0) break;
+      const float x[5] = {v[k].x, v[k].y, v[k].z, v[k].w, w[k]};
+#pragma unroll
+      for (int f = 0; f < 5; ++f) {
+        const float y = x[f] - cmp[f];
+        const float tt = sum[f] + y;
+        cmp[f] = (tt - sum[f]) - y;
+        sum[f] = tt;
+      }
+    }
+  }
+  const float sc = use_invMl ? m.invMl[p] : 1.f;
+#pragma unroll
+  for (int f = 0; f < 5; ++f) out_soa.p[f][p] = sum[f] * sc;
 }
 
 }  // namespace sod

@@ -82,6 +82,7 @@ struct sod_gpu_ctx {
     int nparam = 0, nblk_bwd = 148, step = 0, NP = 0;
     float *params = nullptr, *m1 = nullptr, *m2 = nullptr, *part = nullptr, *grad = nullptr;
     int *pt = nullptr, *pptr = nullptr, *pslot = nullptr;   // patch table [E][NP]; node -> patch-slot CSR
+    int *pos = nullptr;                                      // CSR position of each patch slot [E][NP]
     float *feat = nullptr, *gains = nullptr;                  // [E][8], [E][32]
     float *X = nullptr, *W = nullptr, *Y = nullptr, *SA = nullptr, *dS = nullptr;  // training scratch
     double *Dh = nullptr;                                     // D^-1/2
@@ -279,7 +280,8 @@ void gather_res(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener, int acc
   OutPtrs o{};
   const long long N = c->npoin;
   o.p[0] = Rmass; o.p[1] = Rener; o.p[2] = Rmom; o.p[3] = Rmom + N; o.p[4] = Rmom + 2 * N;
-  k_gather<8, 5, false><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, nullptr, o, accumulate, invml);
+  k_gather_res5<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, (long long)c->nelem * c->N, o,
+                                                             accumulate, invml);
 }
 
 }  // namespace
@@ -502,6 +504,38 @@ int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
   return c->finish();
 }
 
+int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *rho_n, const float *rho,
+                               const float *u, const float *Tem, const float *mu_fluid, const float *mu_e,
+                               const float *mu_sgs, float *Rmass, float *Rmom, float *Rener, int initialze,
+                               float fact) {
+  if (!c || !rho_n || !rho || !u || !Tem || !mu_fluid || !mu_e || !Rmass || !Rmom || !Rener)
+    return fail(SOD_GPU_EINVAL, "bad argument");
+  if (rho_n != rho) return fail(SOD_GPU_EINVAL, "rho_n must alias rho (as every reference caller passes)");
+  const long long EN = (long long)c->nelem * c->N;
+  k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
+  if (mu_sgs) {
+    if (!c->musgs_t) {
+      int rc = c->alloc(&c->musgs_t, (size_t)EN);
+      if (rc) return rc;
+    }
+    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+  }
+  RhsArgs A{};
+  A.rho = rho; A.u = u; A.Tem = Tem; A.mu_fluid = mu_fluid;
+  A.mue_t = c->mue_t; A.musgs_t = mu_sgs ? c->musgs_t : nullptr;
+  A.fact_d = fact;
+  Phys saved = c->ph;
+  c->ph.Cp = Cp; c->ph.Prt = Pr;
+  int rc = dispatch(c, [&](auto L) {
+    L.template rhs<MODE_DIFF | MODE_NOLPS, IN_DIFF>(c, A);
+    return 0;
+  });
+  c->ph = saved;
+  if (rc) return rc;
+  gather_res(c, Rmass, Rmom, Rener, initialze ? 0 : 1, 0);
+  return c->finish();
+}
+
 int sod_gpu_set_mu_e(sod_gpu_ctx *c, const float *mu_e) {
   if (!c || !mu_e) return fail(SOD_GPU_EINVAL, "bad argument");
   const long long EN = (long long)c->nelem * c->N;
@@ -642,6 +676,15 @@ int ensure_cg64(sod_gpu_ctx *c) {
 }
 
 constexpr int CG_HIST = 1024;
+
+// grid of the tensor-core patch kernel: one 16-element group per warp at
+// most, and no more blocks than fit on the GPU at once
+template <int P>
+unsigned tc_grid(long long nelem) {
+  const long long groups = (nelem + 15) / 16;
+  const long long b = (groups + TcDims<P>::WARPS - 1) / TcDims<P>::WARPS;
+  return (unsigned)std::min<long long>(std::max<long long>(b, 1), 3 * 148);
+}
 
 int ensure_cg_loop(sod_gpu_ctx *c) {
   auto &G = c->cg;
@@ -970,11 +1013,11 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
         k_cg_update<false><<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.p, G.q, G.Minv, x, G.r,
                                                                       G.z0, G.S, G.hist, CG_HIST, G.gpart,
                                                                       G.ticket, NT.Dh, NT.uf);
-        k_patch_apply_tc<P><<<2 * 148, 128, TcDims<P>::smem(), st>>>(c->nelem, NT.pt, NT.uf, NT.params, NT.gains,
-                                                                     c->slotsB, &G.S->status);
-        k_cg_patch_z<<<cg_blocks(c->npoin, 2), CG_THREADS, 0, st>>>(c->npoin, NT.pptr, NT.pslot, c->slotsB, G.r,
-                                                                    NT.Dh, NT.params, D::O_ALPHA, G.z0, G.S,
-                                                                    G.gpart, G.ticket);
+        k_patch_apply_tc<P><<<tc_grid<P>(c->nelem), 256, TcDims<P>::smem(), st>>>(
+            c->nelem, NT.pt, NT.pos, NT.uf, NT.params, NT.gains, c->slotsB, &G.S->status);
+        k_cg_patch_z<<<cg_blocks(c->npoin, CG_U), CG_THREADS, 0, st>>>(c->npoin, NT.pptr, c->slotsB, G.r, NT.Dh,
+                                                                       NT.params, D::O_ALPHA, G.z0, G.S, G.gpart,
+                                                                       G.ticket);
       }
       k_cg_dir<<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.z0, G.p, G.S);
       return 0;
@@ -1086,10 +1129,10 @@ int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z) {
     using LL = decltype(L);
     constexpr int P = LL::P_;
     using D = NetDims<P>;
-    k_patch_apply_tc<P><<<2 * 148, 128, TcDims<P>::smem(), c->stream>>>(c->nelem, NT.pt, NT.uf, NT.params,
-                                                                        NT.gains, c->slotsB, nullptr);
-    k_patch_gather<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, NT.pptr, NT.pslot, c->slotsB, r, NT.Dh,
-                                                               NT.params, D::O_ALPHA, z);
+    k_patch_apply_tc<P><<<tc_grid<P>(c->nelem), 256, TcDims<P>::smem(), c->stream>>>(
+        c->nelem, NT.pt, NT.pos, NT.uf, NT.params, NT.gains, c->slotsB, nullptr);
+    k_patch_gather_perm<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, NT.pptr, c->slotsB, r, NT.Dh,
+                                                                    NT.params, D::O_ALPHA, z);
     return 0;
   });
   return 0;
@@ -1624,7 +1667,7 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
     const size_t NPt = (size_t)E * NT.NP;
     if ((rc = c->alloc(&NT.params, NT.nparam)) || (rc = c->alloc(&NT.m1, NT.nparam)) ||
         (rc = c->alloc(&NT.m2, NT.nparam)) || (rc = c->alloc(&NT.grad, NT.nparam)) ||
-        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.pt, NPt)) ||
+        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.pt, NPt)) || (rc = c->alloc(&NT.pos, NPt)) ||
         (rc = c->alloc(&NT.pptr, (size_t)c->npoin + 1)) || (rc = c->alloc(&NT.pslot, NPt)) ||
         (rc = c->alloc(&NT.feat, (size_t)E * NET_F)) || (rc = c->alloc(&NT.gains, (size_t)E * NET_K)) ||
         (rc = c->alloc(&NT.Dh, (size_t)c->npoin)) || (rc = c->alloc(&NT.uf, (size_t)c->npoin)) ||
@@ -1650,14 +1693,18 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
     std::vector<int> conn((size_t)E * N), pt;
     CUDA_TRY(cudaMemcpy(conn.data(), c->conn, conn.size() * 4, cudaMemcpyDeviceToHost));
     if ((rc = build_patch_table(c, conn, pt))) return rc;
-    std::vector<int> pptr(c->npoin + 1, 0), pslot(pt.size());
+    std::vector<int> pptr(c->npoin + 1, 0), pslot(pt.size()), pos(pt.size(), -1);
     for (int v : pt)
       if (v >= 0) pptr[v + 1]++;
     for (long long n = 0; n < c->npoin; ++n) pptr[n + 1] += pptr[n];
     std::vector<int> fill(pptr.begin(), pptr.end() - 1);
     for (size_t i = 0; i < pt.size(); ++i)
-      if (pt[i] >= 0) pslot[fill[pt[i]]++] = (int)i;
+      if (pt[i] >= 0) {
+        pos[i] = fill[pt[i]];
+        pslot[fill[pt[i]]++] = (int)i;
+      }
     CUDA_TRY(cudaMemcpy(NT.pt, pt.data(), pt.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(NT.pos, pos.data(), pos.size() * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(NT.pptr, pptr.data(), pptr.size() * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(NT.pslot, pslot.data(), (size_t)pptr[c->npoin] * 4, cudaMemcpyHostToDevice));
     // geometry features, the last two relative to their mesh mean

@@ -58,6 +58,7 @@ SIGNATURES = {
     "sod_gpu_full_convec_ijk": (C.c_int, [VP] + [VP] * 8 + [C.c_int, C.c_float]),
     "sod_gpu_full_proj_ijk": (C.c_int, [VP] + [VP] * 8),
     "sod_gpu_full_diff_stab_ijk": (C.c_int, [VP, C.c_float, C.c_float] + [VP] * 16 + [C.c_int, C.c_float]),
+    "sod_gpu_full_diffusion_ijk": (C.c_int, [VP, C.c_float, C.c_float] + [VP] * 10 + [C.c_int, C.c_float]),
     "sod_gpu_lumped_solver": (C.c_int, [VP, VP, C.c_int]),
     "sod_gpu_updateF": (C.c_int, [VP, VP, VP, VP, VP, C.c_float] + [VP] * 8),
     "sod_gpu_comp_tau": (C.c_int, [VP, VP, VP, VP]),

@@ -154,3 +154,37 @@ def test_op_level_entry_points_compose_to_updateF(gpu):
         print(f"composed {name}: rel L2 = {err:.3e}")
         assert err < TOL, (name, err)
     ctx.close()
+
+
+@pytest.mark.parametrize("porder", [3, 4])
+def test_plain_diffusion_without_lps(gpu, porder):
+    """full_convec_ijk + full_diffusion_ijk (the flag_lps_stab = .false. path
+    of updateF, time_integ_ls.f90:621-626) + lumped_solver equal the oracle's
+    updateF with LPS off."""
+    m, ic, rho, q, E, u, pr, csound = make_case(porder, 4, seed=13)
+    om = O.OracleMesh(m)
+    N = m.npoin
+    mu_e = np.random.default_rng(5).uniform(0.0, 2e-3, m.nelem * m.nnode).astype(np.float32)
+    tau = O.comp_tau(om, csound, u)
+    Rm, Rq, Re = O.rhs(om, O.comp_params(ic, lps=False), rho, q, E, mu_e, ic.mu_factor, tau)
+    ctx = gpu.Context(m, gpu.phys_from_ic(ic))
+    d = {k: dev(v) for k, v in dict(rho=rho, q=q, E=E, mu_e=mu_e, tau=tau).items()}
+    prim = dict(u=zeros(3 * N), pr=zeros(N), Tem=zeros(N), mu=zeros(N))
+    tmp = dict(Rm=zeros(N), Rq=zeros(3 * N), Re=zeros(N))
+    ctx.call("sod_gpu_updateF", gpu.dptr(d["rho"]), gpu.dptr(d["q"]), gpu.dptr(d["E"]), gpu.dptr(d["mu_e"]),
+             float(ic.mu_factor), gpu.dptr(d["tau"]), gpu.dptr(tmp["Rm"]), gpu.dptr(tmp["Rq"]), gpu.dptr(tmp["Re"]),
+             gpu.dptr(prim["u"]), gpu.dptr(prim["pr"]), gpu.dptr(prim["Tem"]), gpu.dptr(prim["mu"]))
+    h = (prim["pr"] * float(ic.gamma / (ic.gamma - 1.0)) / d["rho"]).contiguous()
+    R = dict(Rm=zeros(N), Rq=zeros(3 * N), Re=zeros(N))
+    ctx.call("sod_gpu_full_convec_ijk", gpu.dptr(prim["u"]), gpu.dptr(d["q"]), gpu.dptr(d["rho"]),
+             gpu.dptr(prim["pr"]), gpu.dptr(h), gpu.dptr(R["Rm"]), gpu.dptr(R["Rq"]), gpu.dptr(R["Re"]), 1, -1.0)
+    ctx.call("sod_gpu_full_diffusion_ijk", float(ic.Cp), float(ic.Prt), gpu.dptr(d["rho"]), gpu.dptr(d["rho"]),
+             gpu.dptr(prim["u"]), gpu.dptr(prim["Tem"]), gpu.dptr(prim["mu"]), gpu.dptr(d["mu_e"]), None,
+             gpu.dptr(R["Rm"]), gpu.dptr(R["Rq"]), gpu.dptr(R["Re"]), 0, -1.0)
+    for k, nc in (("Rm", 1), ("Re", 1), ("Rq", 3)):
+        ctx.call("sod_gpu_lumped_solver", gpu.dptr(R[k]), nc)
+    for name, a, b in (("mass", R["Rm"], Rm), ("mom", R["Rq"], Rq), ("ener", R["Re"], Re)):
+        err = rel_l2(a.cpu().numpy(), b)
+        print(f"no-LPS {name}: rel L2 = {err:.3e}")
+        assert err < TOL, (name, err)
+    ctx.close()
