@@ -19,7 +19,7 @@
 #define SOD_VEC_XI 1
 #endif
 #ifndef SOD_RHS_MINB
-#define SOD_RHS_MINB 6
+#define SOD_RHS_MINB 7
 #endif
 
 namespace sod {
@@ -143,7 +143,10 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
     sm[el][2][t] = u0; sm[el][3][t] = u1; sm[el][4][t] = u2;
   }
   __syncthreads();
-  if (!active) return;
+  // the element's 12-wide slots are staged in shared memory and written
+  // out with coalesced 16-byte stores
+  __shared__ __align__(16) float ost[EPB * N * 12];
+  if (active) {
   const int i = t % N1, j = (t / N1) % N1, k = t / (N1 * N1);
   float Di[N1], Dj[N1], Dk[N1];
 #pragma unroll
@@ -169,7 +172,7 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
 #pragma unroll
     for (int b = 0; b < 3; ++b) gradU[a][b] = He[b] * gU[a][0] + He[b + 3] * gU[a][1] + He[b + 6] * gU[a][2];
   const float divU = gradU[0][0] + gradU[1][1] + gradU[2][2];
-  float4 *o = reinterpret_cast<float4 *>(slots + (e * N + t) * 12);
+  float4 *o = reinterpret_cast<float4 *>(ost + (el * N + t) * 12);
   float tau[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
@@ -180,6 +183,13 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
   o[0] = make_float4(gv * tau[0][0], gv * tau[0][1], gv * tau[0][2], gv * tau[1][1]);
   o[1] = make_float4(gv * tau[1][2], gv * tau[2][2], gv * gradRho[0], gv * gradRho[1]);
   o[2] = make_float4(gv * gradRho[2], gv * gradT[0], gv * gradT[1], gv * gradT[2]);
+  }
+  __syncthreads();
+  const long long e0 = (long long)blockIdx.x * EPB;
+  const long long ne = (m.nelem - e0) < EPB ? (m.nelem - e0) : EPB;
+  const float4 *src = reinterpret_cast<const float4 *>(ost);
+  float4 *dst = reinterpret_cast<float4 *>(slots + e0 * N * 12);
+  for (int q = threadIdx.x; q < ne * N * 3; q += blockDim.x) dst[q] = src[q];
 }
 
 // ---------------------------------------------------------------------
@@ -241,8 +251,14 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   NodeQ s;
   float mu = 0.f;
   int node = 0;
+  float He[9], gv = 0.f;
   if (active) {
     node = m.conn[e * N + t];
+    // geometry loads issued before the staging barrier (independent of it)
+    const float *g = m.geo + e * 10 * N + t;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) He[c] = g[c * N];
+    gv = g[9 * N];
     if (IN == IN_CONS) {
       eos(ph, Rgas, A.mu_factor, A.rho[node], A.q[node], A.q[node + NP], A.q[node + 2 * NP], A.E[node], s);
       mu = s.mu;
@@ -283,16 +299,11 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   __syncthreads();
   const int i = t % N1, j = (t / N1) % N1, k = t / (N1 * N1);
   float Di[N1], Dj[N1], Dk[N1];
-  float He[9], gv = 0.f;
   float res[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // mass, energy, mom x,y,z
   float gradRho[3], gradU[3][3];
   if (active) {
 #pragma unroll
     for (int q = 0; q < N1; ++q) { Di[q] = m.Dnat[i * N1 + q]; Dj[q] = m.Dnat[j * N1 + q]; Dk[q] = m.Dnat[k * N1 + q]; }
-    const float *g = m.geo + e * 10 * N + t;
-#pragma unroll
-    for (int c = 0; c < 9; ++c) He[c] = g[c * N];
-    gv = g[9 * N];
     float(*f)[N] = sm[el];
     float a0, a1, a2;
     iso_grad<P>(f[F_RHO], i, j, k, Di, Dj, Dk, a0, a1, a2);
