@@ -868,19 +868,20 @@ __global__ void k_sub_mean(int npoin_w, const int *__restrict__ lpoin_w, const d
   b[lpoin_w[t]] -= sum_in[0] / (double)npoin_w;
 }
 
-__global__ void k_ones_dot(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ b,
-                           double *__restrict__ part) {
-  // part reused: single-block deterministic sum of b over working nodes
-  __shared__ double sh[1024];
+// per-block partial sums of b over the working nodes (fixed order); the
+// final sum over blocks is k_dot_final
+__global__ void k_sum_partial(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ b,
+                              double *__restrict__ part) {
+  __shared__ double sh[DOT_THREADS];
   double s = 0.0;
-  for (int t = threadIdx.x; t < npoin_w; t += blockDim.x) s += b[lpoin_w[t]];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npoin_w; t += gridDim.x * blockDim.x) s += b[lpoin_w[t]];
   sh[threadIdx.x] = s;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[0] = sh[0];
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
 __global__ void k_jacobi64(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ Minv,
@@ -922,7 +923,8 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
   k_inv_diag64<<<nblk(N, 256), 256, 0, st>>>((long long)N, G.diag, G.Minv);
   // b := b_in with its mean removed (range of the periodic Laplacian)
   CUDA_TRY(cudaMemcpyAsync(G.b, b_in, N * 8, cudaMemcpyDeviceToDevice, st));
-  k_ones_dot<<<1, 1024, 0, st>>>(nw, c->lpoin_w, G.b, G.dots + 7);
+  k_sum_partial<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(nw, c->lpoin_w, G.b, G.part);
+  k_dot_final<<<1, 1024, 0, st>>>(1, G.part, G.dots + 7);
   k_sub_mean<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.dots + 7, G.b);
   dots<double, 1>(c, DotArgs<double, 1>{{G.b}, {G.b}, {nullptr}}, G.dots + 6);
   double hb;
