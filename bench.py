@@ -40,6 +40,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 B_PER_NODE_STAGE = 402.0
+# DRAM bytes (read + write) of one RHS evaluation per working node, from one
+# ncu capture of the four RHS kernels on the 32^3 workload (548,663,296 B for
+# 884,736 working nodes; profiles/rhs_kernels_64cube_p3.md), scaled by the
+# working nodes of the benchmarked mesh.
+DRAM_B_PER_NODE_STAGE = 548663296 / 884736
 NELEM_1D = 64
 PORDER = 3
 
@@ -387,7 +392,9 @@ def main():
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic", "config": workload_config(),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "frac": round(achieved / peak, 4),
+                     "traffic": int(round(DRAM_B_PER_NODE_STAGE * m.npoin_w)),
+                     "traffic_source": "ncu dram__bytes_read+write of the 4 RHS kernels at 32^3, scaled by working nodes",
                      "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                      "unit_of_work": "one fused RHS evaluation (4 launches): 402 B x working nodes"},
         "e2e": {"value": round(e2e_val, 2), "unit": "Mnode-stages/s", "h2d_bytes_per_step": h2d,
