@@ -49,6 +49,24 @@ NELEM_1D = 64
 PORDER = 3
 
 
+def max_over_ranks(ms: float, world: int, device: str) -> float:
+    """Time of the slowest rank (every rank calls this collectively)."""
+    if world == 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world: int, units_per_rank: int, steps: int, ms: float) -> float:
+    """Whole-job rate in millions of units per second: every rank processes
+    units_per_rank units per step (replicas, weak scaling); ms is the time of
+    the slowest rank."""
+    return world * units_per_rank * steps / (ms / 1e3) / 1e6
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -58,29 +76,61 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples SM clocks and clock-event (throttle) reasons during the timed
+    region: NVML every 10 ms (read-only queries), else nvidia-smi every
+    200 ms."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.sm, self.mx, self.reasons = [], [], set()
         self._stop = threading.Event()
         self._t = None
+        self.source = "nvidia-smi"
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self._bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                          pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+            self.source = "nvml"
+        except Exception:
+            self._nv = None
+
+    def _sample_nvml(self):
+        nv, h = self._nv, self._h
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+        self.mx.append(float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)))
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        for name, bit in zip(self.NAMES, self._bits):
+            if r & bit:
+                self.reasons.add(name)
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        parts = [x.strip() for x in out.stdout.strip().split(",")]
+        if len(parts) >= 7:
+            if parts[0].replace(".", "").isdigit():
+                self.sm.append(float(parts[0]))
+            if parts[1].replace(".", "").isdigit():
+                self.mx.append(float(parts[1]))
+            for i in range(4):
+                if parts[3 + i].lower() == "active":
+                    self.reasons.add(self.NAMES[i])
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                parts = [x.strip() for x in out.stdout.strip().split(",")]
-                if len(parts) >= 7:
-                    self.samples.append(parts)
+                self._sample_nvml() if self._nv else self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.01 if self._nv else 0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -92,14 +142,10 @@ class ClockSampler:
         self._t.join(timeout=10)
 
     def summary(self):
-        if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+        if not self.sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "source": self.source}
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": max(self.mx) if self.mx else None,
+                "reasons": sorted(self.reasons), "samples": len(self.sm), "source": self.source}
 
 
 def build_workload(nelem_1d: int, seed: int = 2024):
@@ -175,7 +221,7 @@ def run_reference(args, rank, world):
     return 0
 
 
-def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_steps=300, lr=1e-3):
+def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_steps=300, lr=1e-3, capacity=256):
     """Pressure-Poisson solve to a 1e-8 FP64-certified relative residual on
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG against the learned
@@ -196,7 +242,7 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
     ctxs = [gpu.Context(m, gpu.default_phys()) for _ in range(2)]
     for c in ctxs:
         c.call("sod_gpu_incomp_init", gpu.dptr(u0), nu)
-    ctxs[0].call("sod_gpu_precond_init", 2024, 256)
+    ctxs[0].call("sod_gpu_precond_init", 2024, capacity)
     st = gpu.SolveStats()
     for k in range(harvest_steps):
         for i, c in enumerate(ctxs):
@@ -219,13 +265,84 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
             fb += st.fallback
         res[name] = {"mean_iterations": round(float(np.mean(it)), 1), "mean_solve_ms": round(float(np.mean(ms)), 3),
                      "max_true_residual": rmax, "fallbacks": fb}
+    dev_bytes = [c.device_bytes for c in ctxs]
     for c in ctxs:
         c.close()
-    return {"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
+    return {"harvest_capacity": capacity, "device_bytes_jacobi_ctx": dev_bytes[1], "device_bytes_learned_ctx": dev_bytes[0],
+            "torch_peak_bytes": int(torch.cuda.max_memory_allocated()),"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
                         f"projection-step pressure systems, FP64-certified tol 1e-8",
             "harvest_steps": harvest_steps, "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
             "final_training_loss": round(float(loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],
             "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3)}
+
+
+def time_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3):
+    """Full compressible time steps (sod_gpu_comp_rk_ls_step: `stages` RHS
+    evaluations, the FP64 low-storage stage updates and, once per step, the
+    entropy-viscosity chain) on the Taylor-Green initial state of a periodic
+    cube nelem1d^3 HEX64, Ma=0.1, at the CFL 0.5 dt of the first step."""
+    import torch
+    from sod2d_b200 import gpu, host
+    m = host.periodic_cube(PORDER, nelem1d)
+    ic = host.tgv_comp_init(m, Ma=0.1)
+    sv = gpu.CompSolver(m, ic, stages=stages, fp64_state=True)
+    for _ in range(warmup):
+        sv.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sv.step()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sv.close()
+    return {"workload": f"compressible TGV time step, periodic cube {nelem1d}^3 HEX64 (p=3), Ma=0.1, "
+                        f"{stages}-stage SSP RK, FP64 state, entropy viscosity + LPS",
+            "ms_per_step": round(ms, 4), "stages": stages,
+            "Mnode_stages_per_s": round(m.npoin_w * stages / (ms / 1e3) / 1e6, 2), "steps_timed": steps}
+
+
+def precision_study(nelem1d=16, nsteps=200, porder=3, Ma=0.1, stages=4):
+    """Compressible TGV (periodic cube nelem1d^3, order porder, Ma, SSP RK
+    with `stages` stages, CFL 0.5, LPS and entropy viscosity on) run three
+    ways from the same initial state: the FP64 oracle (reference arithmetic
+    in double precision), the GPU with FP32 element kernels and FP64 RK
+    state, and the GPU all-FP32.  Reports the relative L2 error of the final
+    rho, rho*u and E and the largest relative error of the kinetic-energy and
+    dissipation histories against the FP64 run."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from sod2d_b200 import gpu, host
+    m = host.periodic_cube(porder, nelem1d)
+    ic = host.tgv_comp_init(m, Ma=Ma)
+    t0 = time.perf_counter()
+    ref_hist, ref_fin = O.tgv_comp_run(O.OracleMesh(m, np.float64), ic, O.comp_params(ic, stages=stages), nsteps)
+    t_ref = time.perf_counter() - t0
+    w = m.lpoin_w - 1
+    N = m.npoin
+    rl2 = lambda a, b: float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+    out = {"workload": f"compressible TGV, periodic cube {nelem1d}^3 HEX{(porder + 1) ** 3}, Ma={Ma}, Re=1600, "
+                       f"{stages}-stage SSP RK, CFL 0.5, {nsteps} steps, LPS + entropy viscosity",
+           "reference": f"oracle in FP64 ({t_ref:.1f} s on the host)"}
+    for name, fp64 in (("fp32_kernels_fp64_state", True), ("all_fp32", False)):
+        sv = gpu.CompSolver(m, ic, stages=stages, fp64_state=fp64)
+        hist = sv.run(nsteps)
+        fin = sv.state()
+        sv.close()
+        q = fin["q"].reshape(3, N)[:, w]
+        qr = ref_fin["q"].reshape(3, N)[:, w]
+        rows = min(len(hist), len(ref_hist))
+        # history errors relative to each column's peak (eps_D starts at zero)
+        relh = np.abs(hist[:rows] - ref_hist[:rows]).max(0) / np.abs(ref_hist[:rows]).max(0)
+        out[name] = {"rel_l2_rho": rl2(fin["rho"][w], ref_fin["rho"][w]), "rel_l2_rhou": rl2(q, qr),
+                     "rel_l2_E": rl2(fin["E"][w], ref_fin["E"][w]),
+                     "EK_err_over_peak": float(relh[1]), "eps_S_err_over_peak": float(relh[2]),
+                     "eps_D_err_over_peak": float(relh[3]), "eps_T_err_over_peak": float(relh[4]),
+                     "history_rows": rows,
+                     "eps_D_peak_over_eps_T_peak": float(np.abs(ref_hist[:rows, 3]).max() /
+                                                         np.abs(ref_hist[:rows, 4]).max())}
+    return out
 
 
 def workload_config():
@@ -252,16 +369,27 @@ def main():
     ap.add_argument("--p-harvest", type=int, default=40)
     ap.add_argument("--p-compare", type=int, default=20)
     ap.add_argument("--p-train", type=int, default=300)
+    ap.add_argument("--p-capacity", type=int, default=256, help="harvested (r, e) pairs kept for training")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="run only the FP32/FP64 precision study against the FP64 oracle (prints its JSON object)")
+    ap.add_argument("--ps-nelem1d", type=int, default=16)
+    ap.add_argument("--ps-steps", type=int, default=200)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     pkw = dict(nelem1d=args.p_nelem1d, harvest_steps=args.p_harvest, compare_steps=args.p_compare,
-               train_steps=args.p_train)
+               train_steps=args.p_train, capacity=args.p_capacity)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.precision_study:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps({"precision_study": precision_study(args.ps_nelem1d, args.ps_steps)}))
+        return 0
     if args.pressure_only:
         if rank == 0:
             import torch
@@ -314,13 +442,11 @@ def main():
         ev1.synchronize()
     ms = ev0.elapsed_time(ev1)
     torch.cuda.synchronize()
-    t_ms = torch.tensor([ms], device="cuda", dtype=torch.float64)
     if world > 1:
         dist.barrier()
-        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
-    ms = float(t_ms.item())
+    ms = max_over_ranks(ms, world, "cuda")
     ms_step = ms / args.steps
-    value = world * m.npoin_w * args.steps / (ms / 1e3) / 1e6  # Mnode-stages/s, all ranks
+    value = job_throughput(world, m.npoin_w, args.steps, ms)  # Mnode-stages/s, all ranks
 
     # end-to-end through the C-ABI with pinned host buffers: every step
     # uploads its state (H2D), evaluates one RHS and downloads the residuals
@@ -374,10 +500,7 @@ def main():
     s_dn.wait_stream(stream)
     e1.record(s_dn)
     e1.synchronize()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_val = world * m.npoin_w * e2e_steps / (float(e2e_ms.item()) / 1e3) / 1e6
+    e2e_val = job_throughput(world, m.npoin_w, e2e_steps, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
     h2d = sum(t.numel() * 4 for t in h_in)
     d2h = sum(t.numel() * 4 for t in h_out[0])
     # the pipelined result must equal the device-resident one
@@ -407,6 +530,7 @@ def main():
     }
     ctx.close()
     if rank == 0 and world == 1 and not args.no_pressure:
+        line["time_step"] = time_step_leg(args.nelem1d)
         line["pressure_solve"] = pressure_leg(**pkw)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = CpuBaseline().sample()

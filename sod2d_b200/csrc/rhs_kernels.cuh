@@ -129,8 +129,14 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
   const long long e = (long long)blockIdx.x * EPB + el;
   const bool active = (e < m.nelem) && (t < N);
   const long long NP = m.npoin;
+  float He[9], gv = 0.f;
   if (active) {
     const int node = m.conn[e * N + t];
+    // geometry loads issued before the staging barrier (independent of it)
+    const float *g = m.geo + e * 10 * N + t;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) He[c] = g[c * N];
+    gv = g[9 * N];
     float rho, u0, u1, u2, T;
     if (PRIM) {  // a0 = rho, a1 = u(N,3), a2 = Tem
       rho = a0[node]; u0 = a1[node]; u1 = a1[node + NP]; u2 = a1[node + 2 * NP]; T = a2[node];
@@ -151,11 +157,6 @@ k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float
   float Di[N1], Dj[N1], Dk[N1];
 #pragma unroll
   for (int s = 0; s < N1; ++s) { Di[s] = m.Dnat[i * N1 + s]; Dj[s] = m.Dnat[j * N1 + s]; Dk[s] = m.Dnat[k * N1 + s]; }
-  const float *g = m.geo + e * 10 * N + t;
-  float He[9];
-#pragma unroll
-  for (int c = 0; c < 9; ++c) He[c] = g[c * N];
-  const float gv = g[9 * N];
   float gR[3], gT[3], gU[3][3];
   iso_grad<P>(sm[el][0], i, j, k, Di, Dj, Dk, gR[0], gR[1], gR[2]);
   iso_grad<P>(sm[el][1], i, j, k, Di, Dj, Dk, gT[0], gT[1], gT[2]);
