@@ -253,9 +253,12 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
     ctxs[0].call("sod_gpu_precond_train", train_steps, 16, lr, 7, C.byref(loss))
     train_s = time.perf_counter() - t0
     res = {}
+    uu = torch.zeros(3 * N, device="cuda")
+    div = torch.zeros(N, device="cuda")
+    w = torch.from_numpy((m.lpoin_w - 1).astype(np.int64)).cuda()
     for i, (name, kind) in enumerate((("jacobi", 0), ("learned", 1))):
         c = ctxs[0] if kind == 1 else ctxs[1]
-        it, ms, rmax, fb = [], [], 0.0, 0
+        it, ms, rmax, fb, dv = [], [], 0.0, 0, []
         for k in range(compare_steps):
             o = gpu.SolveOpts(50000, 1e-8, kind, 200, 0)
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
@@ -263,17 +266,23 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
             ms.append(st.seconds * 1e3)
             rmax = max(rmax, st.res_rel)
             fb += st.fallback
+            # velocity divergence after the projection: L2 norm of the assembled int N div u
+            c.call("sod_gpu_incomp_get", gpu.dptr(uu), None)
+            c.call("sod_gpu_eval_divergence", gpu.dptr(uu), gpu.dptr(div))
+            dv.append(float(div[w].double().norm()))
         res[name] = {"mean_iterations": round(float(np.mean(it)), 1), "mean_solve_ms": round(float(np.mean(ms)), 3),
-                     "max_true_residual": rmax, "fallbacks": fb}
+                     "max_true_residual": rmax, "fallbacks": fb, "mean_div_u_l2": float(np.mean(dv))}
     dev_bytes = [c.device_bytes for c in ctxs]
     for c in ctxs:
         c.close()
-    return {"harvest_capacity": capacity, "device_bytes_jacobi_ctx": dev_bytes[1], "device_bytes_learned_ctx": dev_bytes[0],
-            "torch_peak_bytes": int(torch.cuda.max_memory_allocated()),"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
+    return {"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
                         f"projection-step pressure systems, FP64-certified tol 1e-8",
-            "harvest_steps": harvest_steps, "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
+            "harvest_steps": harvest_steps, "compare_steps": compare_steps, "harvest_capacity": capacity,
+            "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
             "final_training_loss": round(float(loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],
-            "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3)}
+            "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3),
+            "device_bytes_jacobi_ctx": dev_bytes[1], "device_bytes_learned_ctx": dev_bytes[0],
+            "torch_peak_bytes": int(torch.cuda.max_memory_allocated())}
 
 
 def time_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3):

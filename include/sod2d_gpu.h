@@ -235,9 +235,11 @@ int sod_gpu_precond_harvest_count(sod_gpu_ctx *ctx);
 int sod_gpu_precond_train(sod_gpu_ctx *ctx, int steps, int batch, float lr, uint64_t seed, float *final_loss);
 
 /* ---- incompressible projection step (pressure-system generator) --------
- * A first-order explicit projection step of the periodic incompressible
- * Navier-Stokes equations built from the operators above:
- *   u* = u - dt (C(u) + nu L u) / Ml   (C: full_convec_ijk_incomp, L: Laplacian)
+ * An explicit projection step of the periodic incompressible Navier-Stokes
+ * equations built from the operators above, with third-order Adams-Bashforth
+ * for the explicit terms (first and second order on the first two steps):
+ *   F^n = (C(u) + nu L u) / Ml        (C: full_convec_ijk_incomp, L: Laplacian)
+ *   u* = u - dt (23/12 F^n - 16/12 F^(n-1) + 5/12 F^(n-2))
  *   A p = -div(u*)/dt,  p0 = 2 p^n - p^(n-1) (extrapolated from the previous
  *   two pressures), solved by sod_gpu_pressure_solve
  *   u = u* - dt grad p

@@ -100,6 +100,7 @@ struct sod_gpu_ctx {
   struct Inc {
     bool ready = false;
     float *u = nullptr, *ustar = nullptr, *R = nullptr, *L = nullptr, *div = nullptr, *grad = nullptr, *pf = nullptr;
+    float *F[3] = {nullptr, nullptr, nullptr};  // explicit tendencies of the last three steps
     double *p = nullptr, *pold = nullptr, *b = nullptr, *x = nullptr;
     double nu = 0.0;
     int nsteps = 0;
@@ -1850,16 +1851,25 @@ int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64
 namespace {
 
 // u* = u - dt (R + nu L) * invMl over working nodes (3 components)
+// explicit tendency F = (R + nu L) / Ml of this step, and the Adams-Bashforth
+// predictor u* = u - dt (c0 F^n + c1 F^(n-1) + c2 F^(n-2)) over working nodes
 __global__ void k_predictor(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
                             const float *__restrict__ invMl, const float *__restrict__ u, const float *__restrict__ R,
-                            const float *__restrict__ L, float dt, float nu, float *__restrict__ us) {
+                            const float *__restrict__ L, float nu, float *__restrict__ Fn,
+                            const float *__restrict__ Fm1, const float *__restrict__ Fm2, float c0, float c1, float c2,
+                            float dt, float *__restrict__ us) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
   const long long i = lpoin_w[t];
   const float im = invMl[i];
   for (int d = 0; d < 3; ++d) {
     const long long k = i + npoin * d;
-    us[k] = u[k] - dt * (R[k] + nu * L[k]) * im;
+    const float f = (R[k] + nu * L[k]) * im;
+    Fn[k] = f;
+    float g = c0 * f;
+    if (c1 != 0.f) g = g + c1 * Fm1[k];
+    if (c2 != 0.f) g = g + c2 * Fm2[k];
+    us[k] = u[k] - dt * g;
   }
 }
 
@@ -1900,12 +1910,13 @@ int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
     if ((rc = c->alloc(&I.u, 3 * N)) || (rc = c->alloc(&I.ustar, 3 * N)) || (rc = c->alloc(&I.R, 3 * N)) ||
         (rc = c->alloc(&I.L, 3 * N)) || (rc = c->alloc(&I.div, N)) || (rc = c->alloc(&I.grad, 3 * N)) ||
         (rc = c->alloc(&I.pf, N)) || (rc = c->alloc(&I.p, N)) || (rc = c->alloc(&I.pold, N)) ||
-        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)))
+        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)) || (rc = c->alloc(&I.F[0], 3 * N)) ||
+        (rc = c->alloc(&I.F[1], 3 * N)) || (rc = c->alloc(&I.F[2], 3 * N)))
       return rc;
     I.ready = true;
   }
   CUDA_TRY(cudaMemcpyAsync(I.u, u, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
-  for (float *z : {I.ustar, I.R, I.L, I.grad}) CUDA_TRY(cudaMemsetAsync(z, 0, 3 * N * 4, c->stream));
+  for (float *z : {I.ustar, I.R, I.L, I.grad, I.F[0], I.F[1], I.F[2]}) CUDA_TRY(cudaMemsetAsync(z, 0, 3 * N * 4, c->stream));
   for (double *z : {I.p, I.pold, I.b, I.x}) CUDA_TRY(cudaMemsetAsync(z, 0, N * 8, c->stream));
   CUDA_TRY(cudaMemsetAsync(I.div, 0, N * 4, c->stream));
   CUDA_TRY(cudaMemsetAsync(I.pf, 0, N * 4, c->stream));
@@ -1928,7 +1939,13 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
     lap<float>(c, I.u + N * d, I.L + N * d);
   }
   if (rc) { c->async = was_async; return rc; }
-  k_predictor<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->invMl, I.u, I.R, I.L, dt, (float)I.nu, I.ustar);
+  // third-order Adams-Bashforth (first and second order for the first two steps)
+  const int sl = I.nsteps % 3;
+  float cab[3] = {1.f, 0.f, 0.f};
+  if (I.nsteps == 1) { cab[0] = 1.5f; cab[1] = -0.5f; }
+  if (I.nsteps >= 2) { cab[0] = 23.f / 12.f; cab[1] = -16.f / 12.f; cab[2] = 5.f / 12.f; }
+  k_predictor<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->invMl, I.u, I.R, I.L, (float)I.nu, I.F[sl],
+                                         I.F[(sl + 2) % 3], I.F[(sl + 1) % 3], cab[0], cab[1], cab[2], dt, I.ustar);
   rc = sod_gpu_eval_divergence(c, I.ustar, I.div);
   if (rc) { c->async = was_async; return rc; }
   // initial guess: the previous pressure for Jacobi (the reference's x0,
