@@ -221,15 +221,16 @@ def run_reference(args, rank, world):
     return 0
 
 
-def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_steps=300, lr=1e-3, capacity=256):
+def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, train_steps=300, lr=1e-3, capacity=256):
     """Pressure-Poisson solve to a 1e-8 FP64-certified relative residual on
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG against the learned
     element-patch preconditioner, each on its own trajectory of the
     projection-step driver from the same initial velocity.  The first
-    `harvest_steps` steps run Jacobi and harvest (residual, error) pairs;
-    the network is then trained on the GPU; the next `compare_steps` solves
-    are timed on both trajectories (device time of each solve)."""
+    `harvest_steps` steps (200) run Jacobi and harvest (residual, error)
+    pairs; the network is then trained on the GPU; the next `compare_steps`
+    solves (800) are timed on both trajectories (device time of each solve),
+    with the velocity divergence after each projection."""
     import ctypes as C
     import torch
     from sod2d_b200 import gpu, host
@@ -271,7 +272,9 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
             c.call("sod_gpu_eval_divergence", gpu.dptr(uu), gpu.dptr(div))
             dv.append(float(div[w].double().norm()))
         res[name] = {"mean_iterations": round(float(np.mean(it)), 1), "mean_solve_ms": round(float(np.mean(ms)), 3),
-                     "max_true_residual": rmax, "fallbacks": fb, "mean_div_u_l2": float(np.mean(dv))}
+                     "max_true_residual": rmax, "fallbacks": fb, "mean_div_u_l2": float(np.mean(dv)),
+                     "mean_solve_ms_first_100": round(float(np.mean(ms[:100])), 3),
+                     "iterations_every_50_steps": it[::50]}
     dev_bytes = [c.device_bytes for c in ctxs]
     for c in ctxs:
         c.close()
@@ -281,6 +284,8 @@ def pressure_leg(nelem1d=32, harvest_steps=40, compare_steps=20, dt=0.01, train_
             "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
             "final_training_loss": round(float(loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],
             "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3),
+            "speedup_wall_first_100_steps": round(res["jacobi"]["mean_solve_ms_first_100"] /
+                                                  res["learned"]["mean_solve_ms_first_100"], 3),
             "device_bytes_jacobi_ctx": dev_bytes[1], "device_bytes_learned_ctx": dev_bytes[0],
             "torch_peak_bytes": int(torch.cuda.max_memory_allocated())}
 
@@ -375,8 +380,8 @@ def main():
     ap.add_argument("--pressure-only", action="store_true",
                     help="run only the pressure-solve comparison (prints its JSON object)")
     ap.add_argument("--p-nelem1d", type=int, default=32)
-    ap.add_argument("--p-harvest", type=int, default=40)
-    ap.add_argument("--p-compare", type=int, default=20)
+    ap.add_argument("--p-harvest", type=int, default=200)
+    ap.add_argument("--p-compare", type=int, default=800)
     ap.add_argument("--p-train", type=int, default=300)
     ap.add_argument("--p-capacity", type=int, default=256, help="harvested (r, e) pairs kept for training")
     ap.add_argument("--precision-study", action="store_true",
