@@ -234,6 +234,29 @@ int sod_gpu_precond_harvest_count(sod_gpu_ctx *ctx);
  * pairs; *final_loss (host) = mean loss of the last batch. */
 int sod_gpu_precond_train(sod_gpu_ctx *ctx, int steps, int batch, float lr, uint64_t seed, float *final_loss);
 
+/* ---- implicit velocity solve of the incompressible step -----------------
+ * species_tau, src/lib_species/sources/elem_stab_species.f90:122-148:
+ * tau(nelem) = max over element nodes of helem (c_species_stab/p) |u|. */
+int sod_gpu_species_tau(sod_gpu_ctx *ctx, const float *u, float *tau);
+/* eval_tau_veloc, src/lib_sod2d_incomp/sources/mod_operators.f90:373-483:
+ * GradX/Y/Z(npoin,3) = assembled gpvol (grad u + grad u^T) rows / Ml. */
+int sod_gpu_eval_tau_veloc(sod_gpu_ctx *ctx, const float *u, float *GradX, float *GradY, float *GradZ);
+/* full_diff_stab_incomp, src/lib_sod2d_incomp/sources/elem_stab_incomp.f90:
+ * 12-153: Rmom(npoin,3) (overwritten) = assembled weak divergence of
+ * (mu_fluid + mu_sgs + tau)(grad u + grad u^T) - tau TauP; mu_sgs is
+ * (nelem,ngaus) and may be NULL (zero). */
+int sod_gpu_full_diff_stab_incomp(sod_gpu_ctx *ctx, const float *u, const float *mu_fluid, const float *mu_sgs,
+                                  const float *TauPX, const float *TauPY, const float *TauPZ,
+                                  const float *tau_stab, float *Rmom);
+/* conjGrad_veloc_incomp (LPS path, periodic mesh),
+ * src/lib_sod2d_incomp/sources/mod_solver_incomp.f90:27-251: preconditioned
+ * CG on Ml x + fact dt D(x) = R, D = full_diff_stab_incomp with the LPS
+ * projection of its argument, preconditioner Ml/dt, x0 = Rp0, tau from
+ * species_tau(Rp0); FP32 vectors, FP64 dots, the reference's arithmetic.
+ * R (npoin,3): in the right-hand side, out the solution. */
+int sod_gpu_conjgrad_veloc(sod_gpu_ctx *ctx, float fact, float dt, const float *mu_fluid, const float *mu_sgs,
+                           const float *Rp0, float *R, int maxIter, double tol, int *iters, double *res_rel);
+
 /* ---- incompressible projection step (pressure-system generator) --------
  * An explicit projection step of the periodic incompressible Navier-Stokes
  * equations built from the operators above, with third-order Adams-Bashforth

@@ -72,6 +72,13 @@ def lib() -> C.CDLL:
                                                                  [C.c_int, C.c_double, C.c_void_p, C.c_void_p])
             getattr(_lib, f"oracle_cg_pressure_{s}").restype = C.c_int
             getattr(_lib, f"oracle_analysis_{s}").argtypes = ([C.POINTER(MeshT), C.c_double] + [C.c_void_p] * 5)
+            real = C.c_float if s == "f32" else C.c_double
+            for nm, na in (("species_tau", 2), ("eval_tau_veloc", 2), ("full_diff_stab_incomp", 6)):
+                getattr(_lib, f"oracle_{nm}_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * na
+                getattr(_lib, f"oracle_{nm}_{s}").restype = C.c_int
+            getattr(_lib, f"oracle_cg_veloc_{s}").argtypes = ([C.POINTER(MeshT), real, real] + [C.c_void_p] * 4 +
+                                                              [C.c_int, C.c_double, C.c_void_p])
+            getattr(_lib, f"oracle_cg_veloc_{s}").restype = C.c_int
     return _lib
 
 
@@ -198,6 +205,42 @@ def cg_pressure(om, diag, x0, rhs, maxIter=20, tol=1e-2):
     keep = [c(diag), c(x0), c(rhs)]
     it = om.fn("cg_pressure")(C.byref(om.s), *(_p(a) for a in keep), maxIter, tol, _p(out), C.byref(res))
     return out, it, res.value
+
+
+def species_tau(om, u):
+    """species_tau: element stabilisation time tau (nelem,) from u (N,3)."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = np.zeros(om.mesh.nelem, om.dtype)
+    keep = c(u)
+    om.fn("species_tau")(C.byref(om.s), _p(keep), _p(out))
+    return out
+
+
+def eval_tau_veloc(om, u):
+    """eval_tau_veloc: (GradX, GradY, GradZ), each (N,3) flattened, mass-inverted."""
+    out = _op(om, "eval_tau_veloc", 9, u)
+    N = om.mesh.npoin
+    return out[:3 * N], out[3 * N:6 * N], out[6 * N:]
+
+
+def full_diff_stab_incomp(om, u, mu_fluid, mu_sgs, tauP, tau_stab):
+    """full_diff_stab_incomp: Rmom (N,3) flattened; tauP = GradX|GradY|GradZ."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = np.zeros(3 * om.mesh.npoin, om.dtype)
+    keep = [c(u), c(mu_fluid), c(mu_sgs), c(tauP), c(tau_stab)]
+    om.fn("full_diff_stab_incomp")(C.byref(om.s), *(_p(a) for a in keep), _p(out))
+    return out
+
+
+def cg_veloc(om, fact, dt, mu_fluid, mu_sgs, Rp0, b, maxIter=20, tol=1e-2):
+    """conjGrad_veloc_incomp (LPS path): returns (x, iterations, ||r||/||r0||)."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    rio = c(b).copy()
+    res = C.c_double()
+    keep = [c(mu_fluid), c(mu_sgs), c(Rp0)]
+    it = om.fn("cg_veloc")(C.byref(om.s), float(fact), float(dt), *(_p(a) for a in keep), _p(rio), maxIter, tol,
+                           C.byref(res))
+    return rio, it, res.value
 
 
 def comp_tau(om: OracleMesh, csound, u):

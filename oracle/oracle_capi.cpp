@@ -514,4 +514,35 @@ ORACLE_BOTH(DEF_FIRST)
   }
 ORACLE_BOTH(DEF_INCOMP)
 
+#define DEF_VELOC(R, S)                                                                                \
+  int oracle_species_tau_##S(const oracle_mesh_t *cm, const R *u, R *tau) {                            \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    species_tau<R>(m, u, g.helem, tau);                                                                \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_eval_tau_veloc_##S(const oracle_mesh_t *cm, const R *u, R *out) {                         \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    const long long N = m.npoin;                                                                       \
+    eval_tau_veloc<R>(m, g, u, out, out + 3 * N, out + 6 * N);                                         \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_full_diff_stab_incomp_##S(const oracle_mesh_t *cm, const R *u, const R *mu_fluid,         \
+                                       const R *mu_sgs, const R *tauP, const R *tau_stab, R *out) {    \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    const long long N = m.npoin;                                                                       \
+    full_diff_stab_incomp<R>(m, g, u, mu_fluid, mu_sgs, tauP, tauP + 3 * N, tauP + 6 * N, tau_stab,    \
+                             out);                                                                     \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_cg_veloc_##S(const oracle_mesh_t *cm, R fact, R dt, const R *mu_fluid, const R *mu_sgs,   \
+                          const R *Rp0, R *Rio, int maxIter, double tol, double *res) {                \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    return conjGrad_veloc<R>(m, g, fact, dt, g.helem, mu_fluid, mu_sgs, Rp0, Rio, maxIter, tol, res);  \
+  }
+ORACLE_BOTH(DEF_VELOC)
+
 }  // extern "C"

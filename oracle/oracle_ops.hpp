@@ -948,4 +948,198 @@ int conjGrad_pressure(const Mesh &m, const Geo<R> &g, const R *diag, const R *x0
   return iter > maxIter ? maxIter : iter;
 }
 
+// ---- species_tau, src/lib_species/sources/elem_stab_species.f90:122-148
+// tau_e = max over the element nodes of helem_k * (c_species_stab / p) * |u|.
+template <class R>
+void species_tau(const Mesh &m, const R *u, const R *helem_k, R *tau, R c_species_stab = R(0.5)) {
+  const long long N = m.npoin;
+  Idx ix(m);
+  for (long long e = 0; e < m.nelem; ++e) {
+    R taul = 0;
+    for (int a = 0; a < m.nnode; ++a) {
+      const int p = ix.node(e, a);
+      const R uu = u[p] * u[p] + u[p + N] * u[p + N] + u[p + 2 * N] * u[p + 2 * N];
+      const R aux1 = std::sqrt(uu);
+      taul = std::max(taul, helem_k[e] * (c_species_stab / R(m.porder)) * aux1);
+    }
+    tau[e] = taul;
+  }
+}
+
+// Velocity gradient at one Gauss point: gradU(i,j) = sum_k He(j,k) d_k u_i.
+template <class R>
+inline void grad_u(const Mesh &m, const Geo<R> &g, const Idx &ix, long long e, int gp, const R *ul, R gradU[3][3]) {
+  const int I = m.gI[gp] - 1, J = m.gJ[gp] - 1, K = m.gK[gp] - 1;
+  R gU[3][3] = {};
+  for (int ii = 0; ii < m.np1; ++ii) {
+    const int an[3] = {ix.inv(ii, J, K), ix.inv(I, ii, K), ix.inv(I, J, ii)};
+    for (int i = 0; i < 3; ++i)
+      for (int d = 0; d < 3; ++d) gU[i][d] = gU[i][d] + DL(g, m, gp, d, ii) * ul[an[d] * 3 + i];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      gradU[i][j] = 0;
+      for (int k = 0; k < 3; ++k) gradU[i][j] = gradU[i][j] + HE(g, m, j, k, gp, e) * gU[i][k];
+    }
+}
+
+// ---- eval_tau_veloc, src/lib_sod2d_incomp/sources/mod_operators.f90:373-483
+// GradX/Y/Z(:,d) = (sum_e gpvol (grad u + grad u^T)(row, d)) / Ml.
+template <class R>
+void eval_tau_veloc(const Mesh &m, const Geo<R> &g, const R *u, R *GX, R *GY, R *GZ) {
+  const long long N = m.npoin;
+  const int n = m.nnode;
+  for (long long p = 0; p < 3 * N; ++p) { GX[p] = 0; GY[p] = 0; GZ[p] = 0; }
+  std::vector<R> buf((size_t)m.nelem * n * 9);
+  Idx ix(m);
+#pragma omp parallel for schedule(static)
+  for (long long e = 0; e < m.nelem; ++e) {
+    std::vector<R> ul(n * 3);
+    for (int a = 0; a < n; ++a) {
+      const int p = ix.node(e, a);
+      for (int d = 0; d < 3; ++d) ul[a * 3 + d] = u[p + N * d];
+    }
+    for (int gp = 0; gp < n; ++gp) {
+      R gradU[3][3];
+      grad_u(m, g, ix, e, gp, ul.data(), gradU);
+      R *b = &buf[((size_t)e * n + gp) * 9];
+      const R gv = GV(g, m, gp, e);
+      for (int d = 0; d < 3; ++d) {
+        b[d] = gv * (gradU[0][d] + gradU[d][0]);
+        b[3 + d] = gv * (gradU[1][d] + gradU[d][1]);
+        b[6 + d] = gv * (gradU[2][d] + gradU[d][2]);
+      }
+    }
+  }
+  R *dst[9] = {GX, GX + N, GX + 2 * N, GY, GY + N, GY + 2 * N, GZ, GZ + N, GZ + 2 * N};
+  scatter(m, buf, 9, dst, R(1));
+  for (int t = 0; t < m.npoin_w; ++t) {  // lumped_solver_vect: R / Ml
+    const int p = m.lpoin_w[t] - 1;
+    for (int c = 0; c < 9; ++c) dst[c][p] = dst[c][p] / g.Ml[p];
+  }
+}
+
+// ---- full_diff_stab_incomp, src/lib_sod2d_incomp/sources/elem_stab_incomp.f90:12-153
+// Rmom = sum_e weak div of (mu_fluid + mu_sgs + tau_e)(grad u + grad u^T)
+// - tau_e TauP (Rmom is zeroed first).
+template <class R>
+void full_diff_stab_incomp(const Mesh &m, const Geo<R> &g, const R *u, const R *mu_fluid, const R *mu_sgs,
+                           const R *TPX, const R *TPY, const R *TPZ, const R *tau_stab, R *Rmom) {
+  const long long N = m.npoin, NE = m.nelem;
+  const int n = m.nnode;
+  for (long long p = 0; p < 3 * N; ++p) Rmom[p] = 0;
+  std::vector<R> buf((size_t)m.nelem * n * 3);
+  Idx ix(m);
+#pragma omp parallel for schedule(static)
+  for (long long e = 0; e < m.nelem; ++e) {
+    std::vector<R> ul(n * 3), mufl(n), musgs(n), tpx(n * 3), tpy(n * 3), tpz(n * 3);
+    std::vector<R> tauX(n * 3), tauY(n * 3), tauZ(n * 3);
+    for (int a = 0; a < n; ++a) {
+      const int p = ix.node(e, a);
+      mufl[a] = mu_fluid[p];
+      musgs[a] = mu_sgs[e + NE * a];
+      for (int d = 0; d < 3; ++d) {
+        ul[a * 3 + d] = u[p + N * d];
+        tpx[a * 3 + d] = TPX[p + N * d]; tpy[a * 3 + d] = TPY[p + N * d]; tpz[a * 3 + d] = TPZ[p + N * d];
+      }
+    }
+    const R ts = tau_stab[e];
+    for (int gp = 0; gp < n; ++gp) {
+      const R mu_fgp = mufl[gp] + musgs[gp] + ts;
+      R gradU[3][3];
+      grad_u(m, g, ix, e, gp, ul.data(), gradU);
+      R tau[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) tau[i][j] = gradU[i][j] + gradU[j][i];
+      for (int d = 0; d < 3; ++d) {
+        tauX[gp * 3 + d] = mu_fgp * tau[0][d] - ts * tpx[gp * 3 + d];
+        tauY[gp * 3 + d] = mu_fgp * tau[1][d] - ts * tpy[gp * 3 + d];
+        tauZ[gp * 3 + d] = mu_fgp * tau[2][d] - ts * tpz[gp * 3 + d];
+      }
+    }
+    for (int gp = 0; gp < n; ++gp) {
+      R *b = &buf[((size_t)e * n + gp) * 3];
+      b[0] = weak_div(m, g, ix, e, gp, tauX.data());
+      b[1] = weak_div(m, g, ix, e, gp, tauY.data());
+      b[2] = weak_div(m, g, ix, e, gp, tauZ.data());
+    }
+  }
+  R *dst[3] = {Rmom, Rmom + N, Rmom + 2 * N};
+  scatter(m, buf, 3, dst, R(1));
+}
+
+// ---- conjGrad_veloc_incomp (LPS path, periodic), src/lib_sod2d_incomp/sources/mod_solver_incomp.f90:27-251
+// Preconditioned CG on Ml x + fact dt D(x) = b, D = full_diff_stab_incomp
+// with the LPS projection of its argument, preconditioner Ml / dt, x0 = Rp0,
+// tau from species_tau(x0); vectors in R, dots in FP64 (node-major order),
+// alpha and beta rounded to R.  Rio: in b (npoin,3), out x.  Returns the
+// iteration count; *res_rel = ||r|| / ||r0|| at exit.
+template <class R>
+int conjGrad_veloc(const Mesh &m, const Geo<R> &g, R fact, R dt, const R *helem_k, const R *mu_fluid,
+                   const R *mu_sgs, const R *Rp0, R *Rio, int maxIter, double tol, double *res_rel) {
+  const long long N = m.npoin;
+  std::vector<R> x(Rp0, Rp0 + 3 * N), r0(3 * N, 0), p0(3 * N, 0), qn(3 * N, 0), b(Rio, Rio + 3 * N), z0(3 * N, 0),
+      z1(3 * N, 0), Mu(3 * N, 0), tau(m.nelem), TX(3 * N), TY(3 * N), TZ(3 * N);
+  for (long long p = 0; p < N; ++p)
+    for (int d = 0; d < 3; ++d) Mu[p + N * d] = g.Ml[p] / dt;
+  species_tau(m, x.data(), helem_k, tau.data());
+  auto apply = [&](const R *v) {
+    eval_tau_veloc(m, g, v, TX.data(), TY.data(), TZ.data());
+    full_diff_stab_incomp(m, g, v, mu_fluid, mu_sgs, TX.data(), TY.data(), TZ.data(), tau.data(), qn.data());
+    for (int t = 0; t < m.npoin_w; ++t) {
+      const int p = m.lpoin_w[t] - 1;
+      for (int d = 0; d < 3; ++d) qn[p + N * d] = v[p + N * d] * g.Ml[p] + qn[p + N * d] * fact * dt;
+    }
+  };
+  apply(x.data());
+  for (int t = 0; t < m.npoin_w; ++t) {
+    const int p = m.lpoin_w[t] - 1;
+    for (int d = 0; d < 3; ++d) r0[p + N * d] = b[p + N * d] - qn[p + N * d];
+  }
+  for (int t = 0; t < m.npoin_w; ++t) {
+    const int p = m.lpoin_w[t] - 1;
+    for (int d = 0; d < 3; ++d) { z0[p + N * d] = r0[p + N * d] / Mu[p + N * d]; p0[p + N * d] = z0[p + N * d]; }
+  }
+  auto dot = [&](auto f) {
+    double s = 0.0;
+    for (int t = 0; t < m.npoin_w; ++t) {
+      const int p = m.lpoin_w[t] - 1;
+      for (int d = 0; d < 3; ++d) s += f(p + N * d);
+    }
+    return s;
+  };
+  const double auxB = std::sqrt(dot([&](long long k) { return (double)(r0[k] * r0[k]); }));
+  double nrm = auxB;
+  int iter;
+  for (iter = 1; iter <= maxIter; ++iter) {
+    apply(p0.data());
+    const double Q1 = dot([&](long long k) { return (double)(r0[k] * z0[k]); });
+    const double Q2 = dot([&](long long k) { return (double)(p0[k] * qn[k]); });
+    const R alpha = (R)(Q1 / Q2);
+    for (int t = 0; t < m.npoin_w; ++t) {
+      const int p = m.lpoin_w[t] - 1;
+      for (int d = 0; d < 3; ++d) x[p + N * d] = x[p + N * d] + alpha * p0[p + N * d];
+    }
+    for (int t = 0; t < m.npoin_w; ++t) {
+      const int p = m.lpoin_w[t] - 1;
+      for (int d = 0; d < 3; ++d) r0[p + N * d] = r0[p + N * d] - alpha * qn[p + N * d];
+    }
+    for (int t = 0; t < m.npoin_w; ++t) {
+      const int p = m.lpoin_w[t] - 1;
+      for (int d = 0; d < 3; ++d) { z1[p + N * d] = z0[p + N * d]; z0[p + N * d] = r0[p + N * d] / Mu[p + N * d]; }
+    }
+    nrm = std::sqrt(dot([&](long long k) { return (double)(r0[k] * r0[k]); }));
+    if (nrm < tol * auxB) break;
+    const double T = dot([&](long long k) { return (double)(r0[k] * (z0[k] - z1[k])); });
+    const R beta = (R)(T / Q1);
+    for (int t = 0; t < m.npoin_w; ++t) {
+      const int p = m.lpoin_w[t] - 1;
+      for (int d = 0; d < 3; ++d) p0[p + N * d] = z0[p + N * d] + beta * p0[p + N * d];
+    }
+  }
+  for (long long k = 0; k < 3 * N; ++k) Rio[k] = x[k];
+  *res_rel = auxB > 0 ? nrm / auxB : 0.0;
+  return iter > maxIter ? maxIter : iter;
+}
+
 }  // namespace oracle

@@ -5,6 +5,7 @@
 #include "step_kernels.cuh"
 #include "incomp_kernels.cuh"
 #include "precond_net.cuh"
+#include "veloc_kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -105,6 +106,11 @@ struct sod_gpu_ctx {
     double nu = 0.0;
     int nsteps = 0;
   } inc;
+  // implicit velocity solve (conjGrad_veloc_incomp)
+  struct Velo {
+    float *tauP = nullptr, *tau_e = nullptr;                   // [npoin][8] projection, [E] tau
+    float *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *z1 = nullptr, *b = nullptr;  // (npoin,3)
+  } velo;
   // compressible time-integration state
   struct Comp {
     bool ready = false, fp64 = true, first = true;
@@ -1900,6 +1906,167 @@ __global__ void k_corrector(int npoin_w, long long npoin, const int *__restrict_
 }  // namespace
 
 extern "C" {
+
+}  // extern "C"
+
+// ---- implicit velocity solve (conjGrad_veloc_incomp) ----------------------
+
+namespace {
+
+int ensure_velo(sod_gpu_ctx *c) {
+  auto &V = c->velo;
+  if (V.tauP) return 0;
+  const size_t N = c->npoin;
+  int rc;
+  if ((rc = c->alloc(&V.tauP, N * 8)) || (rc = c->alloc(&V.tau_e, (size_t)c->nelem)) ||
+      (rc = c->alloc(&V.x, 3 * N)) || (rc = c->alloc(&V.r, 3 * N)) || (rc = c->alloc(&V.p, 3 * N)) ||
+      (rc = c->alloc(&V.q, 3 * N)) || (rc = c->alloc(&V.z, 3 * N)) || (rc = c->alloc(&V.z1, 3 * N)) ||
+      (rc = c->alloc(&V.b, 3 * N)))
+    return rc;
+  if (!c->cg.part && ((rc = c->alloc(&c->cg.part, 8 * DOT_BLOCKS)) || (rc = c->alloc(&c->cg.dots, 16)))) return rc;
+  for (float *v : {V.x, V.r, V.p, V.q, V.z, V.z1, V.b}) CUDA_TRY(cudaMemsetAsync(v, 0, 3 * N * 4, c->stream));
+  return 0;
+}
+
+// LPS projection of v into V.tauP (node-major, mass-divided)
+void velo_tau(sod_gpu_ctx *c, const float *v) {
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_tauv_elem<LL::P_, LL::EPB><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), v, c->slotsB);
+    return 0;
+  });
+  k_gather_tauv<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, c->Ml, c->velo.tauP);
+}
+
+// out (npoin,3) = full_diff_stab_incomp(v) with the projection in V.tauP
+void velo_diff(sod_gpu_ctx *c, const float *v, const float *mu_fluid, const float *musgs_t, const float *tau_e,
+               float *out) {
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_diffv_elem<LL::P_, LL::EPB><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), v, mu_fluid, musgs_t,
+                                                                                c->velo.tauP, tau_e, c->slotsB);
+    return 0;
+  });
+  OutPtrs o{};
+  const long long N = c->npoin;
+  o.p[0] = out; o.p[1] = out + N; o.p[2] = out + 2 * N;
+  k_gather<4, 3, false><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, nullptr, o, 0, 0);
+}
+
+// FP64 sums of the products of two (npoin,3) vectors (two pairs at once)
+int velo_dots(sod_gpu_ctx *c, const float *a0, const float *b0, const float *c0, const float *a1, const float *b1,
+              double *h) {
+  const long long N = c->npoin;
+  DotArgs<float, 6> A{};
+  for (int d = 0; d < 3; ++d) {
+    A.a[d] = a0 + N * d; A.b[d] = b0 + N * d; A.c[d] = c0 ? c0 + N * d : nullptr;
+    A.a[3 + d] = a1 ? a1 + N * d : a0 + N * d; A.b[3 + d] = b1 ? b1 + N * d : b0 + N * d; A.c[3 + d] = nullptr;
+  }
+  dots<float, 6>(c, A, c->cg.dots + 8);
+  double t[6];
+  CUDA_TRY(cudaMemcpyAsync(t, c->cg.dots + 8, 48, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  h[0] = (t[0] + t[1]) + t[2];
+  h[1] = (t[3] + t[4]) + t[5];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sod_gpu_species_tau(sod_gpu_ctx *c, const float *u, float *tau) {
+  if (!c || !u || !tau) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (!c->helem) return fail(SOD_GPU_EINVAL, "species_tau needs helem at init");
+  k_species_tau<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->nelem, c->N, c->conn, c->helem, u, c->npoin,
+                                                          c->phys.c_species_stab / (float)c->P, tau);
+  return c->finish();
+}
+
+int sod_gpu_eval_tau_veloc(sod_gpu_ctx *c, const float *u, float *GradX, float *GradY, float *GradZ) {
+  if (!c || !u || !GradX || !GradY || !GradZ) return fail(SOD_GPU_EINVAL, "bad argument");
+  int rc;
+  if ((rc = ensure_velo(c))) return rc;
+  velo_tau(c, u);
+  k_unpack_tauv<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, c->velo.tauP, GradX, GradY, GradZ);
+  return c->finish();
+}
+
+int sod_gpu_full_diff_stab_incomp(sod_gpu_ctx *c, const float *u, const float *mu_fluid, const float *mu_sgs,
+                                  const float *TauPX, const float *TauPY, const float *TauPZ, const float *tau_stab,
+                                  float *Rmom) {
+  if (!c || !u || !mu_fluid || !TauPX || !TauPY || !TauPZ || !tau_stab || !Rmom)
+    return fail(SOD_GPU_EINVAL, "bad argument");
+  int rc;
+  if ((rc = ensure_velo(c))) return rc;
+  const long long EN = (long long)c->nelem * c->N;
+  if (mu_sgs) {
+    if (!c->musgs_t && (rc = c->alloc(&c->musgs_t, (size_t)EN))) return rc;
+    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+  }
+  k_pack_tauv<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, TauPX, TauPY, TauPZ, c->velo.tauP);
+  velo_diff(c, u, mu_fluid, mu_sgs ? c->musgs_t : nullptr, tau_stab, Rmom);
+  return c->finish();
+}
+
+int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu_fluid, const float *mu_sgs,
+                           const float *Rp0, float *R, int maxIter, double tol, int *iters, double *res_rel) {
+  if (!c || !mu_fluid || !Rp0 || !R || maxIter < 1 || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (!c->helem) return fail(SOD_GPU_EINVAL, "conjgrad_veloc needs helem at init");
+  int rc;
+  if ((rc = ensure_velo(c))) return rc;
+  auto &V = c->velo;
+  const long long N = c->npoin, EN = (long long)c->nelem * c->N;
+  const int nw = c->npoin_w;
+  const unsigned nb = nblk(nw, 256);
+  const bool was_async = c->async;
+  c->async = true;
+  const float *musgs = nullptr;
+  if (mu_sgs) {
+    if (!c->musgs_t && (rc = c->alloc(&c->musgs_t, (size_t)EN))) return rc;
+    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+    musgs = c->musgs_t;
+  }
+  CUDA_TRY(cudaMemcpyAsync(V.x, Rp0, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(V.b, R, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  k_species_tau<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->nelem, c->N, c->conn, c->helem, V.x, N,
+                                                          c->phys.c_species_stab / (float)c->P, V.tau_e);
+  auto apply = [&](const float *v) {  // q = v Ml + fact dt D(v)
+    velo_tau(c, v);
+    velo_diff(c, v, mu_fluid, musgs, V.tau_e, V.q);
+    k_veloc_op<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, v, fact, dt, V.q);
+  };
+  apply(V.x);
+  k_veloc_vec<<<nb, 256, 0, c->stream>>>(0, nw, N, c->lpoin_w, c->Ml, dt, 0.f, 0.f, V.b, V.x, V.r, V.p, V.q, V.z,
+                                         V.z1);
+  double h[2];
+  if ((rc = velo_dots(c, V.r, V.r, nullptr, nullptr, nullptr, h))) { c->async = was_async; return rc; }
+  const double auxB = std::sqrt(h[0]);
+  double nrm = auxB;
+  int it;
+  for (it = 1; it <= maxIter; ++it) {
+    apply(V.p);
+    if ((rc = velo_dots(c, V.r, V.z, nullptr, V.p, V.q, h))) { c->async = was_async; return rc; }
+    const double Q1 = h[0];
+    const float alpha = (float)(h[0] / h[1]);
+    k_veloc_vec<<<nb, 256, 0, c->stream>>>(1, nw, N, c->lpoin_w, c->Ml, dt, alpha, 0.f, V.b, V.x, V.r, V.p, V.q,
+                                           V.z, V.z1);
+    if ((rc = velo_dots(c, V.r, V.r, nullptr, V.r, V.z, h))) { c->async = was_async; return rc; }
+    nrm = std::sqrt(h[0]);
+    if (!std::isfinite(nrm)) { c->async = was_async; return fail(SOD_GPU_ENONFINITE, "non-finite residual in velocity CG"); }
+    if (nrm < tol * auxB) break;
+    // Polak-Ribiere: r.(z - z1)
+    if ((rc = velo_dots(c, V.r, V.z, V.z1, V.r, V.z, h))) { c->async = was_async; return rc; }
+    const float beta = (float)(h[0] / Q1);
+    k_veloc_vec<<<nb, 256, 0, c->stream>>>(2, nw, N, c->lpoin_w, c->Ml, dt, 0.f, beta, V.b, V.x, V.r, V.p, V.q, V.z,
+                                           V.z1);
+  }
+  CUDA_TRY(cudaMemcpyAsync(R, V.x, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  c->async = was_async;
+  if (iters) *iters = it > maxIter ? maxIter : it;
+  if (res_rel) *res_rel = auxB > 0 ? nrm / auxB : 0.0;
+  return c->finish();
+}
 
 int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
   if (!c || !u || nu < 0) return fail(SOD_GPU_EINVAL, "bad argument");

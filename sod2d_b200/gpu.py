@@ -88,6 +88,11 @@ SIGNATURES = {
     "sod_gpu_incomp_init": (C.c_int, [VP, VP, C.c_double]),
     "sod_gpu_incomp_step": (C.c_int, [VP, C.c_float, VP, VP]),
     "sod_gpu_incomp_get": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_species_tau": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_eval_tau_veloc": (C.c_int, [VP] * 5),
+    "sod_gpu_full_diff_stab_incomp": (C.c_int, [VP] * 9),
+    "sod_gpu_conjgrad_veloc": (C.c_int, [VP, C.c_float, C.c_float, VP, VP, VP, VP, C.c_int, C.c_double,
+                                         C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "sod_gpu_analysis_noalloc": (C.c_int, [C.c_int] * 4 + [VP] * 15 + [C.c_float, C.c_float, VP,
                                                                        C.POINTER(C.c_double)]),
 }
