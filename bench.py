@@ -226,11 +226,12 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG against the learned
     element-patch preconditioner, each on its own trajectory of the
-    projection-step driver from the same initial velocity.  The first
+    BDF3/EXT3 incompressible step (with its implicit velocity solve) from the
+    same initial velocity.  The first
     `harvest_steps` steps (200) run Jacobi and harvest (residual, error)
     pairs; the network is then trained on the GPU; the next `compare_steps`
     solves (800) are timed on both trajectories (device time of each solve),
-    with the velocity divergence after each projection."""
+    with the velocity divergence after each step."""
     import ctypes as C
     import torch
     from sod2d_b200 import gpu, host
@@ -259,7 +260,8 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     w = torch.from_numpy((m.lpoin_w - 1).astype(np.int64)).cuda()
     for i, (name, kind) in enumerate((("jacobi", 0), ("learned", 1))):
         c = ctxs[0] if kind == 1 else ctxs[1]
-        it, ms, rmax, fb, dv = [], [], 0.0, 0, []
+        it, ms, rmax, fb, dv, vits = [], [], 0.0, 0, [], []
+        vit = C.c_int()
         for k in range(compare_steps):
             o = gpu.SolveOpts(50000, 1e-8, kind, 200, 0)
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
@@ -267,11 +269,14 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
             ms.append(st.seconds * 1e3)
             rmax = max(rmax, st.res_rel)
             fb += st.fallback
-            # velocity divergence after the projection: L2 norm of the assembled int N div u
+            # velocity divergence after the step: L2 norm of the assembled int N div u
             c.call("sod_gpu_incomp_get", gpu.dptr(uu), None)
             c.call("sod_gpu_eval_divergence", gpu.dptr(uu), gpu.dptr(div))
             dv.append(float(div[w].double().norm()))
+            c.call("sod_gpu_incomp_veloc_stats", C.byref(vit), None)
+            vits.append(vit.value)
         res[name] = {"mean_iterations": round(float(np.mean(it)), 1), "mean_solve_ms": round(float(np.mean(ms)), 3),
+                     "mean_velocity_cg_iterations": round(float(np.mean(vits)), 2),
                      "max_true_residual": rmax, "fallbacks": fb, "mean_div_u_l2": float(np.mean(dv)),
                      "mean_solve_ms_first_100": round(float(np.mean(ms[:100])), 3),
                      "iterations_every_50_steps": it[::50]}
@@ -279,7 +284,7 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     for c in ctxs:
         c.close()
     return {"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
-                        f"projection-step pressure systems, FP64-certified tol 1e-8",
+                        f"BDF3/EXT3-step pressure systems, FP64-certified tol 1e-8",
             "harvest_steps": harvest_steps, "compare_steps": compare_steps, "harvest_capacity": capacity,
             "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
             "final_training_loss": round(float(loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],

@@ -257,20 +257,28 @@ int sod_gpu_full_diff_stab_incomp(sod_gpu_ctx *ctx, const float *u, const float 
 int sod_gpu_conjgrad_veloc(sod_gpu_ctx *ctx, float fact, float dt, const float *mu_fluid, const float *mu_sgs,
                            const float *Rp0, float *R, int maxIter, double tol, int *iters, double *res_rel);
 
-/* ---- incompressible projection step (pressure-system generator) --------
- * An explicit projection step of the periodic incompressible Navier-Stokes
- * equations built from the operators above, with third-order Adams-Bashforth
- * for the explicit terms (first and second order on the first two steps):
- *   F^n = (C(u) + nu L u) / Ml        (C: full_convec_ijk_incomp, L: Laplacian)
- *   u* = u - dt (23/12 F^n - 16/12 F^(n-1) + 5/12 F^(n-2))
- *   A p = -div(u*)/dt,  p0 = 2 p^n - p^(n-1) (extrapolated from the previous
- *   two pressures), solved by sod_gpu_pressure_solve
- *   u = u* - dt grad p
- * It stands in for the reference's BDF/EXT3 step with its implicit velocity
- * solve (time_integ_incomp.f90:88-434) as a source of the time sequence of
- * pressure-Poisson systems. */
+/* ---- incompressible time step (library-owned state) ---------------------
+ * bdfext3_main_incomp on a periodic mesh without wall model, source term or
+ * LES, src/lib_sod2d_incomp/sources/time_integ_incomp.f90:88-434, rho = 1,
+ * mu_fluid = nu, with BDF coefficients (g0, a) and extrapolation
+ * coefficients (b) of order 1, 2 and 3 on the first, second and later steps:
+ *   Rmom2 = full_convec_ijk_incomp(u1, u1, 1)
+ *   u2 = (-dt (b1 Rmom2 + b2 Rmom1 + b3 Rmom3) / Ml + a1 u1 + a2 u3 + a3 u4) / g0
+ *   A p = -g0 eval_divergence(u2) / dt   solved by sod_gpu_pressure_solve
+ *   u2 = (u2 - dt eval_gradient(p) / g0) Ml
+ *   u2 = sod_gpu_conjgrad_veloc(fact 1/g0, dt, mu_fluid, x0 = u1, R = u2)
+ * then the levels rotate (u4 = u3, u3 = u1, u1 = u2; CFDSolverBase.f90:
+ * 1953-2015).  The pressure solve starts from the previous pressure
+ * (Jacobi, the reference's pr(:,1)) or from 2 p^n - p^(n-1) (learned).
+ * init needs helem (species_tau of the velocity solve) and sets every level
+ * to u. */
 int sod_gpu_incomp_init(sod_gpu_ctx *ctx, const float *u, double nu);
 int sod_gpu_incomp_step(sod_gpu_ctx *ctx, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats);
+/* maxIter and tol of the velocity solve (defaults 20 and 1e-4,
+ * mod_numerical_params.f90:50-51). */
+int sod_gpu_incomp_set_veloc_solver(sod_gpu_ctx *ctx, int maxIter, double tol);
+/* Iterations and ||r||/||r0|| of the last step's velocity solve (host). */
+int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *ctx, int *iters, double *res_rel);
 /* Copies of the current velocity u(npoin,3) (FP32) and pressure (FP64); NULL skips. */
 int sod_gpu_incomp_get(sod_gpu_ctx *ctx, float *u, double *p);
 

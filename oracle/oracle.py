@@ -243,6 +243,92 @@ def cg_veloc(om, fact, dt, mu_fluid, mu_sgs, Rp0, b, maxIter=20, tol=1e-2):
     return rio, it, res.value
 
 
+def _pressure_fp64(om64, b, x0, tol=1e-11, maxIter=5000):
+    """Jacobi-preconditioned CG in FP64 on the assembled Laplacian over the
+    working nodes.  The periodic system is singular (constants) and, with
+    single-precision geometry, its rows sum to ~1e-8 instead of 0, so the
+    right-hand side and every residual are projected to zero mean; without
+    that the iterate drifts along the near-constant null vector once the
+    residual reaches the inconsistency floor (~1e-10)."""
+    w = om64.mesh.lpoin_w - 1
+    A = lambda v: laplacian(om64, v)
+    d = laplacian_diag(om64)
+    b = np.asarray(b, np.float64).copy()
+    b[w] -= b[w].mean()
+    x = np.asarray(x0, np.float64).copy()
+    r = np.zeros_like(b)
+    r[w] = (b - A(x))[w]
+    r[w] -= r[w].mean()
+    z = np.zeros_like(b)
+    z[w] = r[w] / d[w]
+    p = z.copy()
+    rz = float(r[w] @ z[w])
+    bn = float(np.linalg.norm(b[w]))
+    for _ in range(maxIter):
+        if np.linalg.norm(r[w]) <= tol * bn:
+            break
+        q = A(p)
+        a = rz / float(p[w] @ q[w])
+        x[w] += a * p[w]
+        r[w] -= a * q[w]
+        r[w] -= r[w].mean()
+        z[w] = r[w] / d[w]
+        rz_new = float(r[w] @ z[w])
+        p[w] = z[w] + (rz_new / rz) * p[w]
+        rz = rz_new
+    return x
+
+
+class IncompState:
+    """Time levels of bdfext3_main_incomp: u(:,:,1..4), Rmom(:,:,1..3), pr."""
+
+    def __init__(self, u0):
+        u0 = np.asarray(u0, np.float32)
+        self.u1, self.u3, self.u4 = u0.copy(), u0.copy(), u0.copy()
+        self.Rm1 = np.zeros_like(u0)
+        self.Rm3 = np.zeros_like(u0)
+        self.p = np.zeros(u0.size // 3)
+        self.iltime = 1
+
+
+def bdfext3_step(om, om64, st: IncompState, dt, nu, maxIter=20, tol=1e-4):
+    """One bdfext3_main_incomp step (periodic mesh, no wall model, source term
+    or LES; rho = 1, mu_fluid = nu), time_integ_incomp.f90:88-434, composed
+    of the oracle operators above; the pressure system is solved in FP64 to a
+    1e-12 residual.  Updates st in place and returns the velocity solve's
+    (iterations, ||r||/||r0||)."""
+    N = om.mesh.npoin
+    w = om.mesh.lpoin_w - 1
+    f32 = np.float32
+    it = st.iltime
+    if it == 1:
+        g0, a, b = 1.0, (1.0, 0.0, 0.0), (1.0, 0.0, 0.0)
+    elif it == 2:
+        g0, a, b = 1.5, (2.0, -0.5, 0.0), (2.0, -1.0, 0.0)
+    else:
+        g0, a, b = 11.0 / 6.0, (3.0, -1.5, 1.0 / 3.0), (3.0, -3.0, 1.0)
+    g0, a, b = f32(g0), [f32(v) for v in a], [f32(v) for v in b]
+    dt = f32(dt)
+    Rm2 = convec_incomp(om, st.u1, st.u1)
+    Ml = np.tile(np.asarray(om.mesh.Ml, f32), 3)
+    W = np.concatenate([w + N * d for d in range(3)])
+    u2 = np.zeros(3 * N, f32)
+    e = b[0] * Rm2[W] + b[1] * st.Rm1[W] + b[2] * st.Rm3[W]
+    u2[W] = (dt * (-e) / Ml[W] + a[0] * st.u1[W] + a[1] * st.u3[W] + a[2] * st.u4[W]) / g0
+    st.Rm3, st.Rm1 = st.Rm1, Rm2
+    rhs = -np.float64(g0) * divergence(om, u2).astype(np.float64) / np.float64(dt)
+    p = _pressure_fp64(om64, rhs, st.p)
+    gp = gradient(om, p.astype(f32))
+    u2[W] = (u2[W] - dt * gp[W] / g0) * Ml[W]
+    mu = np.full(N, nu, f32)
+    musgs = np.zeros(om.mesh.nelem * om.mesh.nnode, f32)
+    u2, vit, vres = cg_veloc(om, 1.0 / g0, dt, mu, musgs, st.u1, u2, maxIter=maxIter, tol=tol)
+    st.u4, st.u3, st.u1 = st.u3, st.u1, u2
+    st.p = p
+    st.iltime += 1
+    return vit, vres
+
+
 def comp_tau(om: OracleMesh, csound, u):
     out = np.zeros(om.mesh.nelem, om.dtype)
     om.fn("comp_tau")(C.byref(om.s), _p(np.ascontiguousarray(csound, om.dtype)),

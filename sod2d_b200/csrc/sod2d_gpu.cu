@@ -97,14 +97,19 @@ struct sod_gpu_ctx {
     double *xsnap = nullptr;  // solver snapshots (FP64) while harvesting
     double *tmp1 = nullptr, *tmp2 = nullptr;
   } net;
-  // incompressible projection-step state
+  // incompressible BDF3/EXT3 state (time levels rotate by pointer)
   struct Inc {
     bool ready = false;
-    float *u = nullptr, *ustar = nullptr, *R = nullptr, *L = nullptr, *div = nullptr, *grad = nullptr, *pf = nullptr;
-    float *F[3] = {nullptr, nullptr, nullptr};  // explicit tendencies of the last three steps
+    float *u[4] = {nullptr, nullptr, nullptr, nullptr};  // u(:,:,1..4): u^n, new level, u^(n-1), u^(n-2)
+    float *Rm[3] = {nullptr, nullptr, nullptr};          // Rmom(:,:,1..3)
+    float *div = nullptr, *grad = nullptr, *pf = nullptr, *mu = nullptr;
     double *p = nullptr, *pold = nullptr, *b = nullptr, *x = nullptr;
     double nu = 0.0;
     int nsteps = 0;
+    int v_maxiter = 20;  // mod_numerical_params.f90:50-51 defaults
+    double v_tol = 1e-4;
+    int v_iters = 0;     // statistics of the last velocity solve
+    double v_res = 0.0;
   } inc;
   // implicit velocity solve (conjGrad_veloc_incomp)
   struct Velo {
@@ -1852,55 +1857,74 @@ int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64
 
 }  // extern "C"
 
-// ---- incompressible projection step -------------------------------------
+// ---- incompressible BDF3/EXT3 step --------------------------------------
 
 namespace {
 
-// u* = u - dt (R + nu L) * invMl over working nodes (3 components)
-// explicit tendency F = (R + nu L) / Ml of this step, and the Adams-Bashforth
-// predictor u* = u - dt (c0 F^n + c1 F^(n-1) + c2 F^(n-2)) over working nodes
-__global__ void k_predictor(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
-                            const float *__restrict__ invMl, const float *__restrict__ u, const float *__restrict__ R,
-                            const float *__restrict__ L, float nu, float *__restrict__ Fn,
-                            const float *__restrict__ Fm1, const float *__restrict__ Fm2, float c0, float c1, float c2,
-                            float dt, float *__restrict__ us) {
+// BDF (gamma0, alpha) and extrapolation (beta) coefficients of the local step
+// iltime (1-based), time_integ_incomp.f90:166-230
+struct BdfCoef {
+  float g0, a[3], b[3];
+};
+
+BdfCoef bdf_coef(int iltime) {
+  if (iltime == 1) return {1.f, {1.f, 0.f, 0.f}, {1.f, 0.f, 0.f}};
+  if (iltime == 2) return {1.5f, {2.f, -0.5f, 0.f}, {2.f, -1.f, 0.f}};
+  return {11.f / 6.f, {3.f, -1.5f, 1.f / 3.f}, {3.f, -3.f, 1.f}};
+}
+
+// u2 = -(b1 Rm2 + b2 Rm1 + b3 Rm3); u2 = (dt u2 / Ml + a1 u1 + a2 u3 + a3 u4) / g0
+// over working nodes, time_integ_incomp.f90:288-305 (terms with a zero
+// coefficient are skipped, so levels not yet filled are never read)
+__global__ void k_bdf_ext(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ Ml,
+                          const float *__restrict__ Rm2, const float *__restrict__ Rm1, const float *__restrict__ Rm3,
+                          const float *__restrict__ u1, const float *__restrict__ u3, const float *__restrict__ u4,
+                          BdfCoef k, float dt, float *__restrict__ u2) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
   const long long i = lpoin_w[t];
-  const float im = invMl[i];
+  const float ml = Ml[i];
   for (int d = 0; d < 3; ++d) {
-    const long long k = i + npoin * d;
-    const float f = (R[k] + nu * L[k]) * im;
-    Fn[k] = f;
-    float g = c0 * f;
-    if (c1 != 0.f) g = g + c1 * Fm1[k];
-    if (c2 != 0.f) g = g + c2 * Fm2[k];
-    us[k] = u[k] - dt * g;
+    const long long j = i + npoin * d;
+    float e = k.b[0] * Rm2[j];
+    if (k.b[1] != 0.f) e = e + k.b[1] * Rm1[j];
+    if (k.b[2] != 0.f) e = e + k.b[2] * Rm3[j];
+    float v = dt * (-e) / ml + k.a[0] * u1[j];
+    if (k.a[1] != 0.f) v = v + k.a[1] * u3[j];
+    if (k.a[2] != 0.f) v = v + k.a[2] * u4[j];
+    u2[j] = v / k.g0;
   }
 }
 
-// b = -div/dt ; x = 2 p - pold (working nodes)
-__global__ void k_poisson_rhs(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ div, float dt,
-                              const double *__restrict__ p, const double *__restrict__ pold, int nhist,
+// b = -g0 div / dt (time_integ_incomp.f90:316-317); x0 = the previous
+// pressure (nhist 1, the reference's pr(:,1)), or 2 p - pold (nhist >= 2)
+__global__ void k_poisson_rhs(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ div, float g0,
+                              float dt, const double *__restrict__ p, const double *__restrict__ pold, int nhist,
                               double *__restrict__ b, double *__restrict__ x) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
   const int i = lpoin_w[t];
-  b[i] = -(double)div[i] / (double)dt;
+  b[i] = -(double)g0 * (double)div[i] / (double)dt;
   x[i] = nhist >= 2 ? 2.0 * p[i] - pold[i] : (nhist == 1 ? p[i] : 0.0);
 }
 
-// u = u* - dt grad p ; pold = p ; p = x ; pf = (float) x
-__global__ void k_corrector(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
-                            const float *__restrict__ us, const float *__restrict__ gp, float dt,
-                            float *__restrict__ u) {
+// u2 = (u2 - dt gradP / g0) Ml, time_integ_incomp.f90:352-358 (no wall model)
+__global__ void k_veloc_rhs(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
+                            const float *__restrict__ Ml, const float *__restrict__ gp, float dt, float g0,
+                            float *__restrict__ u2) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
   const long long i = lpoin_w[t];
+  const float ml = Ml[i];
   for (int d = 0; d < 3; ++d) {
-    const long long k = i + npoin * d;
-    u[k] = us[k] - dt * gp[k];
+    const long long j = i + npoin * d;
+    u2[j] = (u2[j] - dt * gp[j] / g0) * ml;
   }
+}
+
+__global__ void k_fill(long long n, float v, float *__restrict__ a) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) a[t] = v;
 }
 
 }  // namespace
@@ -2070,26 +2094,46 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu
 
 int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
   if (!c || !u || nu < 0) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (!c->helem) return fail(SOD_GPU_EINVAL, "the incompressible step needs helem at init");
   auto &I = c->inc;
   const size_t N = c->npoin;
   int rc;
   if (!I.ready) {
-    if ((rc = c->alloc(&I.u, 3 * N)) || (rc = c->alloc(&I.ustar, 3 * N)) || (rc = c->alloc(&I.R, 3 * N)) ||
-        (rc = c->alloc(&I.L, 3 * N)) || (rc = c->alloc(&I.div, N)) || (rc = c->alloc(&I.grad, 3 * N)) ||
-        (rc = c->alloc(&I.pf, N)) || (rc = c->alloc(&I.p, N)) || (rc = c->alloc(&I.pold, N)) ||
-        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)) || (rc = c->alloc(&I.F[0], 3 * N)) ||
-        (rc = c->alloc(&I.F[1], 3 * N)) || (rc = c->alloc(&I.F[2], 3 * N)))
+    for (auto &a : I.u)
+      if ((rc = c->alloc(&a, 3 * N))) return rc;
+    for (auto &a : I.Rm)
+      if ((rc = c->alloc(&a, 3 * N))) return rc;
+    if ((rc = c->alloc(&I.div, N)) || (rc = c->alloc(&I.grad, 3 * N)) || (rc = c->alloc(&I.pf, N)) ||
+        (rc = c->alloc(&I.mu, N)) || (rc = c->alloc(&I.p, N)) || (rc = c->alloc(&I.pold, N)) ||
+        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)))
       return rc;
     I.ready = true;
   }
-  CUDA_TRY(cudaMemcpyAsync(I.u, u, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
-  for (float *z : {I.ustar, I.R, I.L, I.grad, I.F[0], I.F[1], I.F[2]}) CUDA_TRY(cudaMemsetAsync(z, 0, 3 * N * 4, c->stream));
+  // every level starts from the initial field (CFDSolverPeriodicIncomp.f90:54-66)
+  for (auto &a : I.u) CUDA_TRY(cudaMemcpyAsync(a, u, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  for (auto &a : I.Rm) CUDA_TRY(cudaMemsetAsync(a, 0, 3 * N * 4, c->stream));
+  CUDA_TRY(cudaMemsetAsync(I.grad, 0, 3 * N * 4, c->stream));
   for (double *z : {I.p, I.pold, I.b, I.x}) CUDA_TRY(cudaMemsetAsync(z, 0, N * 8, c->stream));
   CUDA_TRY(cudaMemsetAsync(I.div, 0, N * 4, c->stream));
   CUDA_TRY(cudaMemsetAsync(I.pf, 0, N * 4, c->stream));
+  k_fill<<<nblk((long long)N, 256), 256, 0, c->stream>>>((long long)N, (float)nu, I.mu);  // constant mu_fluid (rho = 1)
   I.nu = nu;
   I.nsteps = 0;
   return c->finish();
+}
+
+int sod_gpu_incomp_set_veloc_solver(sod_gpu_ctx *c, int maxIter, double tol) {
+  if (!c || maxIter < 1 || !(tol > 0.0)) return fail(SOD_GPU_EINVAL, "bad argument");
+  c->inc.v_maxiter = maxIter;
+  c->inc.v_tol = tol;
+  return 0;
+}
+
+int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *c, int *iters, double *res_rel) {
+  if (!c || !c->inc.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
+  if (iters) *iters = c->inc.v_iters;
+  if (res_rel) *res_rel = c->inc.v_res;
+  return 0;
 }
 
 int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats) {
@@ -2098,40 +2142,47 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
   const long long N = c->npoin;
   const int nw = c->npoin_w;
   const unsigned nb = nblk(nw, 256);
+  const BdfCoef k = bdf_coef(I.nsteps + 1);
+  float *const u1 = I.u[0], *const u2 = I.u[1], *const u3 = I.u[2], *const u4 = I.u[3];
   const bool was_async = c->async;
   c->async = true;  // chain the operator calls; synchronise at the end
-  int rc = sod_gpu_full_convec_ijk_incomp(c, I.u, I.u, I.R);
-  for (int d = 0; d < 3 && !rc; ++d) {
-    CUDA_TRY(cudaMemsetAsync(I.L + N * d, 0, N * 4, c->stream));
-    lap<float>(c, I.u + N * d, I.L + N * d);
+  // Rmom(:,:,2) = full_convec_ijk_incomp(u1, u1 rho, rho), rho = 1
+  int rc = sod_gpu_full_convec_ijk_incomp(c, u1, u1, I.Rm[1]);
+  if (rc) { c->async = was_async; return rc; }
+  k_bdf_ext<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, I.Rm[1], I.Rm[0], I.Rm[2], u1, u3, u4, k, dt, u2);
+  {  // Rmom(:,:,3) = Rmom(:,:,1); Rmom(:,:,1) = Rmom(:,:,2)
+    float *t = I.Rm[2];
+    I.Rm[2] = I.Rm[0]; I.Rm[0] = I.Rm[1]; I.Rm[1] = t;
   }
+  rc = sod_gpu_eval_divergence(c, u2, I.div);
   if (rc) { c->async = was_async; return rc; }
-  // third-order Adams-Bashforth (first and second order for the first two steps)
-  const int sl = I.nsteps % 3;
-  float cab[3] = {1.f, 0.f, 0.f};
-  if (I.nsteps == 1) { cab[0] = 1.5f; cab[1] = -0.5f; }
-  if (I.nsteps >= 2) { cab[0] = 23.f / 12.f; cab[1] = -16.f / 12.f; cab[2] = 5.f / 12.f; }
-  k_predictor<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->invMl, I.u, I.R, I.L, (float)I.nu, I.F[sl],
-                                         I.F[(sl + 2) % 3], I.F[(sl + 1) % 3], cab[0], cab[1], cab[2], dt, I.ustar);
-  rc = sod_gpu_eval_divergence(c, I.ustar, I.div);
-  if (rc) { c->async = was_async; return rc; }
-  // initial guess: the previous pressure for Jacobi (the reference's x0,
+  // initial guess: the previous pressure for Jacobi (the reference's pr(:,1),
   // mod_solver_incomp.f90:306); extrapolated from the previous two
   // pressures for the learned path
   const int hist = opts->precond == 1 ? I.nsteps : (I.nsteps > 0 ? 1 : 0);
-  k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, dt, I.p, I.pold, hist, I.b, I.x);
+  k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, k.g0, dt, I.p, I.pold, hist, I.b, I.x);
   c->async = was_async;
   rc = sod_gpu_pressure_solve(c, I.b, I.x, opts, stats);
   if (rc && rc != SOD_GPU_ESTAGNATE) return rc;
   const int solve_rc = rc;
+  {  // pold = p; p = x
+    double *t = I.pold;
+    I.pold = I.p; I.p = I.x; I.x = t;
+  }
   c->async = true;
-  CUDA_TRY(cudaMemcpyAsync(I.pold, I.p, N * 8, cudaMemcpyDeviceToDevice, c->stream));
-  CUDA_TRY(cudaMemcpyAsync(I.p, I.x, N * 8, cudaMemcpyDeviceToDevice, c->stream));
   k_d2f_w<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.p, I.pf);
   rc = sod_gpu_eval_gradient(c, I.pf, I.grad);
+  if (rc) { c->async = was_async; return rc; }
+  k_veloc_rhs<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, I.grad, dt, k.g0, u2);
   c->async = was_async;
+  int vit = 0;
+  double vres = 0.0;
+  rc = sod_gpu_conjgrad_veloc(c, 1.f / k.g0, dt, I.mu, nullptr, u1, u2, I.v_maxiter, I.v_tol, &vit, &vres);
   if (rc) return rc;
-  k_corrector<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, I.ustar, I.grad, dt, I.u);
+  I.v_iters = vit;
+  I.v_res = vres;
+  // u(:,:,4) = u(:,:,3); u(:,:,3) = u(:,:,1); u(:,:,1) = u(:,:,2) (CFDSolverBase.f90:1953-2015)
+  I.u[0] = u2; I.u[1] = u4; I.u[2] = u1; I.u[3] = u3;
   I.nsteps++;
   rc = c->finish();
   return rc ? rc : solve_rc;
@@ -2139,7 +2190,7 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
 
 int sod_gpu_incomp_get(sod_gpu_ctx *c, float *u, double *p) {
   if (!c || !c->inc.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
-  if (u) CUDA_TRY(cudaMemcpyAsync(u, c->inc.u, (size_t)c->npoin * 12, cudaMemcpyDeviceToDevice, c->stream));
+  if (u) CUDA_TRY(cudaMemcpyAsync(u, c->inc.u[0], (size_t)c->npoin * 12, cudaMemcpyDeviceToDevice, c->stream));
   if (p) CUDA_TRY(cudaMemcpyAsync(p, c->inc.p, (size_t)c->npoin * 8, cudaMemcpyDeviceToDevice, c->stream));
   return c->finish();
 }

@@ -88,6 +88,8 @@ SIGNATURES = {
     "sod_gpu_incomp_init": (C.c_int, [VP, VP, C.c_double]),
     "sod_gpu_incomp_step": (C.c_int, [VP, C.c_float, VP, VP]),
     "sod_gpu_incomp_get": (C.c_int, [VP, VP, VP]),
+    "sod_gpu_incomp_set_veloc_solver": (C.c_int, [VP, C.c_int, C.c_double]),
+    "sod_gpu_incomp_veloc_stats": (C.c_int, [VP, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "sod_gpu_species_tau": (C.c_int, [VP, VP, VP]),
     "sod_gpu_eval_tau_veloc": (C.c_int, [VP] * 5),
     "sod_gpu_full_diff_stab_incomp": (C.c_int, [VP] * 9),

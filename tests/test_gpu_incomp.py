@@ -108,3 +108,59 @@ def test_fp64_solve_reaches_1e8(gpu, case):
     xs = x.cpu().numpy()[w]
     ps = p.astype(np.float64)[w]
     assert rel_l2(xs - xs.mean(), ps - ps.mean()) < 1e-5
+
+
+def test_bdfext3_step_matches_oracle(gpu):
+    """Five bdfext3_main_incomp steps (first-, second- and third-order
+    coefficients) against the oracle's composition of the same operators:
+    velocity and pressure (up to its constant) to 1e-4 relative L2, the
+    velocity solve's iteration counts within one."""
+    m = host.periodic_cube(3, 4, jitter=0.05, seed=21, ordering=1, elem_shuffle=True)
+    om, om64 = O.OracleMesh(m), O.OracleMesh(m, np.float64)
+    N = m.npoin
+    w = m.lpoin_w - 1
+    x, y, z = (m.coord[i * N:(i + 1) * N].astype(np.float64) for i in range(3))
+    u0 = np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),
+                         0.2 * np.sin(x) * np.sin(y)]).astype(np.float32)
+    nu, dt = 1.0 / 100.0, 0.02
+    ctx = gpu.Context(m, gpu.default_phys())
+    du = dv(u0)
+    ctx.call("sod_gpu_incomp_init", gpu.dptr(du), nu)
+    st = O.IncompState(u0)
+    o = gpu.SolveOpts(4000, 1e-9, 0, 200)
+    s = gpu.SolveStats()
+    uu = torch.zeros(3 * N, device="cuda")
+    pp = torch.zeros(N, dtype=torch.float64, device="cuda")
+    vit, vres = C.c_int(), C.c_double()
+    for step in range(5):
+        ctx.call("sod_gpu_incomp_step", 0.02, C.byref(o), C.byref(s))
+        ctx.call("sod_gpu_incomp_veloc_stats", C.byref(vit), C.byref(vres))
+        rit, rres = O.bdfext3_step(om, om64, st, dt, nu)
+        ctx.call("sod_gpu_incomp_get", gpu.dptr(uu), gpu.dptr(pp))
+        ug = uu.cpu().numpy().reshape(3, N)[:, w]
+        ur = st.u1.reshape(3, N)[:, w]
+        pg, pr = pp.cpu().numpy()[w], st.p[w]
+        eu = rel_l2(ug, ur)
+        ep = rel_l2(pg - pg.mean(), pr - pr.mean())
+        print(f"step {step + 1}: pressure its {s.iterations} res {s.res_rel:.2e}; velocity its gpu {vit.value} "
+              f"oracle {rit} res {vres.value:.2e}/{rres:.2e}; rel L2 u {eu:.2e} p {ep:.2e}")
+        assert s.res_rel < 1e-9
+        assert abs(vit.value - rit) <= 1
+        assert eu < 1e-4 and ep < 1e-4
+    # the step did something: the field moved and the pressure is not trivial
+    assert rel_l2(ug, u0.reshape(3, N)[:, w]) > 1e-3
+    assert np.linalg.norm(pr) > 0
+    ctx.close()
+
+
+def test_incomp_step_arguments(gpu):
+    m = host.periodic_cube(3, 2, seed=3)
+    ctx = gpu.Context(m, gpu.default_phys())
+    with pytest.raises(RuntimeError):
+        ctx.call("sod_gpu_incomp_set_veloc_solver", 0, 1e-4)
+    with pytest.raises(RuntimeError):
+        ctx.call("sod_gpu_incomp_set_veloc_solver", 20, 0.0)
+    ctx.call("sod_gpu_incomp_set_veloc_solver", 30, 1e-5)
+    with pytest.raises(RuntimeError):
+        ctx.call("sod_gpu_incomp_veloc_stats", None, None)  # state not initialised
+    ctx.close()

@@ -96,7 +96,8 @@ def test_trained_network_beats_jacobi(gpu):
     loss = C.c_float()
     ctx.call("sod_gpu_precond_train", 300, 8, 3e-3, 5, C.byref(loss))
     print("Jacobi iterations", its_j, "final training loss", loss.value)
-    # the next pressure system, solved from the same zero initial guess by both
+    # a pressure system of the current flow state (first-order explicit
+    # predictor), solved from the same zero initial guess by both
     uu = torch.zeros(3 * N, device="cuda")
     ctx.call("sod_gpu_incomp_get", gpu.dptr(uu), None)
     R = torch.zeros(3 * N, device="cuda")
