@@ -227,7 +227,7 @@ struct TcDims {
   static constexpr int S1 = KP + 4;                                // B as [mode][slot]: stride = 4 mod 8
   static constexpr int S2 = KP + ((8 - KP % 16) + 16) % 16;        // B as [mode][slot]: stride = 8 or 24 mod 32
   static constexpr int SY = NET_K + 4;                             // Y tile [16][SY]
-  static constexpr int WARPS = 8;
+  static constexpr int WARPS = 16;                                 // one block per SM
   static constexpr int KC = 10;                                    // k-steps whose operands are gathered together
   static constexpr int NC = 10;                                    // output n-tiles whose positions are loaded together
   static constexpr size_t smem() { return (size_t)(NET_K * S1 + NET_K * S2 + WARPS * 16 * SY) * 4; }
@@ -257,7 +257,7 @@ __global__ void k_scale_f32(int npoin_w, const int *__restrict__ lpoin_w, const 
 // pos[e][j] so that the assembly reads each node's contributions
 // contiguously.
 template <int P>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(TcDims<P>::WARPS * 32)
 k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restrict__ pos,
                  const float *__restrict__ uf, const float *__restrict__ prm, const float *__restrict__ gains,
                  float *__restrict__ out, const int *__restrict__ stop) {
@@ -278,7 +278,9 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restr
   __syncthreads();
   const int g = lane >> 2, t = lane & 3;
   const long long ngroups = (nelem + 15) / 16;
-  for (long long grp = (long long)blockIdx.x * T::WARPS + warp; grp < ngroups;
+  // groups dealt round-robin over the blocks, so that every SM holds the
+  // same number of groups to within one
+  for (long long grp = (long long)warp * gridDim.x + blockIdx.x; grp < ngroups;
        grp += (long long)gridDim.x * T::WARPS) {
     const long long ea = grp * 16 + g, eb = ea + 8;
     const bool va = ea < nelem, vb = eb < nelem;

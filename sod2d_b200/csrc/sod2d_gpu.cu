@@ -689,14 +689,27 @@ int ensure_cg64(sod_gpu_ctx *c) {
 
 constexpr int CG_HIST = 1024;
 
-// grid of the tensor-core patch kernel: one 16-element group per warp at
-// most, and no more blocks than fit on the GPU at once
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+      n = 148;
+  }
+  return n;
+}
+
+// grid of the tensor-core patch kernel: one block per SM (the block's
+// registers and shared memory allow one), fewer when there are fewer
+// 16-element groups than SMs
 template <int P>
 unsigned tc_grid(long long nelem) {
   const long long groups = (nelem + 15) / 16;
-  const long long b = (groups + TcDims<P>::WARPS - 1) / TcDims<P>::WARPS;
-  return (unsigned)std::min<long long>(std::max<long long>(b, 1), 3 * 148);
+  return (unsigned)std::min<long long>(std::max<long long>(groups, 1), num_sms());
 }
+constexpr int TC_THREADS = TcDims<3>::WARPS * 32;
+static_assert(TcDims<3>::WARPS == TcDims<4>::WARPS, "one block size for both orders");
 
 int ensure_cg_loop(sod_gpu_ctx *c) {
   auto &G = c->cg;
@@ -1027,7 +1040,7 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
         k_cg_update<false><<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.p, G.q, G.Minv, x, G.r,
                                                                       G.z0, G.S, G.hist, CG_HIST, G.gpart,
                                                                       G.ticket, NT.Dh, NT.uf);
-        k_patch_apply_tc<P><<<tc_grid<P>(c->nelem), 256, TcDims<P>::smem(), st>>>(
+        k_patch_apply_tc<P><<<tc_grid<P>(c->nelem), TC_THREADS, TcDims<P>::smem(), st>>>(
             c->nelem, NT.pt, NT.pos, NT.uf, NT.params, NT.gains, c->slotsB, &G.S->status);
         k_cg_patch_z<<<cg_blocks(c->npoin, CG_U), CG_THREADS, 0, st>>>(c->npoin, NT.pptr, c->slotsB, G.r, NT.Dh,
                                                                        NT.params, D::O_ALPHA, G.z0, G.S, G.gpart,
@@ -1143,7 +1156,7 @@ int apply_precond(sod_gpu_ctx *c, int kind, const double *r, double *z) {
     using LL = decltype(L);
     constexpr int P = LL::P_;
     using D = NetDims<P>;
-    k_patch_apply_tc<P><<<tc_grid<P>(c->nelem), 256, TcDims<P>::smem(), c->stream>>>(
+    k_patch_apply_tc<P><<<tc_grid<P>(c->nelem), TC_THREADS, TcDims<P>::smem(), c->stream>>>(
         c->nelem, NT.pt, NT.pos, NT.uf, NT.params, NT.gains, c->slotsB, nullptr);
     k_patch_gather_perm<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, NT.pptr, c->slotsB, r, NT.Dh,
                                                                     NT.params, D::O_ALPHA, z);
