@@ -259,7 +259,7 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *ctx, float fact, float dt, const float *
 
 /* ---- incompressible time step (library-owned state) ---------------------
  * bdfext3_main_incomp on a periodic mesh without wall model, source term or
- * LES, src/lib_sod2d_incomp/sources/time_integ_incomp.f90:88-434, rho = 1,
+ * LES, src/lib_sod2d_incomp/sources/time_integ_incomp.f90:88-433, rho = 1,
  * mu_fluid = nu, with BDF coefficients (g0, a) and extrapolation
  * coefficients (b) of order 1, 2 and 3 on the first, second and later steps:
  *   Rmom2 = full_convec_ijk_incomp(u1, u1, 1)

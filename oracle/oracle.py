@@ -293,7 +293,7 @@ class IncompState:
 
 def bdfext3_step(om, om64, st: IncompState, dt, nu, maxIter=20, tol=1e-4):
     """One bdfext3_main_incomp step (periodic mesh, no wall model, source term
-    or LES; rho = 1, mu_fluid = nu), time_integ_incomp.f90:88-434, composed
+    or LES; rho = 1, mu_fluid = nu), time_integ_incomp.f90:88-433, composed
     of the oracle operators above; the pressure system is solved in FP64 to a
     1e-12 residual.  Updates st in place and returns the velocity solve's
     (iterations, ||r||/||r0||)."""

@@ -1875,7 +1875,7 @@ int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64
 namespace {
 
 // BDF (gamma0, alpha) and extrapolation (beta) coefficients of the local step
-// iltime (1-based), time_integ_incomp.f90:166-230
+// iltime (1-based), time_integ_incomp.f90:165-229
 struct BdfCoef {
   float g0, a[3], b[3];
 };
@@ -1887,7 +1887,7 @@ BdfCoef bdf_coef(int iltime) {
 }
 
 // u2 = -(b1 Rm2 + b2 Rm1 + b3 Rm3); u2 = (dt u2 / Ml + a1 u1 + a2 u3 + a3 u4) / g0
-// over working nodes, time_integ_incomp.f90:288-305 (terms with a zero
+// over working nodes, time_integ_incomp.f90:322-341 (terms with a zero
 // coefficient are skipped, so levels not yet filled are never read)
 __global__ void k_bdf_ext(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ Ml,
                           const float *__restrict__ Rm2, const float *__restrict__ Rm1, const float *__restrict__ Rm3,
@@ -1909,7 +1909,7 @@ __global__ void k_bdf_ext(int npoin_w, long long npoin, const int *__restrict__ 
   }
 }
 
-// b = -g0 div / dt (time_integ_incomp.f90:316-317); x0 = the previous
+// b = -g0 div / dt (time_integ_incomp.f90:351-353); x0 = the previous
 // pressure (nhist 1, the reference's pr(:,1)), or 2 p - pold (nhist >= 2)
 __global__ void k_poisson_rhs(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ div, float g0,
                               float dt, const double *__restrict__ p, const double *__restrict__ pold, int nhist,
@@ -1921,7 +1921,7 @@ __global__ void k_poisson_rhs(int npoin_w, const int *__restrict__ lpoin_w, cons
   x[i] = nhist >= 2 ? 2.0 * p[i] - pold[i] : (nhist == 1 ? p[i] : 0.0);
 }
 
-// u2 = (u2 - dt gradP / g0) Ml, time_integ_incomp.f90:352-358 (no wall model)
+// u2 = (u2 - dt gradP / g0) Ml, time_integ_incomp.f90:390-394 (no wall model)
 __global__ void k_veloc_rhs(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
                             const float *__restrict__ Ml, const float *__restrict__ gp, float dt, float g0,
                             float *__restrict__ u2) {
