@@ -221,17 +221,21 @@ def run_reference(args, rank, world):
     return 0
 
 
-def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, train_steps=300, lr=1e-3, capacity=256):
+def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, train_steps=300, lr=1e-3, capacity=256,
+                 self_steps=16, ft_steps=200, ft_lr=5e-4, ft_batch=8):
     """Pressure-Poisson solve to a 1e-8 FP64-certified relative residual on
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG against the learned
     element-patch preconditioner, each on its own trajectory of the
     BDF3/EXT3 incompressible step (with its implicit velocity solve) from the
-    same initial velocity.  The first
-    `harvest_steps` steps (200) run Jacobi and harvest (residual, error)
-    pairs; the network is then trained on the GPU; the next `compare_steps`
-    solves (800) are timed on both trajectories (device time of each solve),
-    with the velocity divergence after each step."""
+    same initial velocity.  The first `harvest_steps` steps (200) run Jacobi
+    and harvest (residual, error) pairs; the network is then trained on the
+    GPU.  The next `compare_steps` solves (800) are timed on both
+    trajectories (device time of each solve), with the velocity divergence
+    after each step; on the learned trajectory the first `self_steps` (16)
+    of them also harvest pairs from the learned solver's own iterations, and
+    the network is fine-tuned on those (`ft_steps` Adam steps) before the
+    rest.  Training and fine-tuning time is reported apart from the solves."""
     import ctypes as C
     import torch
     from sod2d_b200 import gpu, host
@@ -258,12 +262,20 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     uu = torch.zeros(3 * N, device="cuda")
     div = torch.zeros(N, device="cuda")
     w = torch.from_numpy((m.lpoin_w - 1).astype(np.int64)).cuda()
+    ft_s, ft_loss, ft_pairs = 0.0, C.c_float(), 0
     for i, (name, kind) in enumerate((("jacobi", 0), ("learned", 1))):
         c = ctxs[0] if kind == 1 else ctxs[1]
         it, ms, rmax, fb, dv, vits = [], [], 0.0, 0, [], []
         vit = C.c_int()
+        if kind == 1 and self_steps > 0:
+            c.call("sod_gpu_precond_restart_harvest")
         for k in range(compare_steps):
-            o = gpu.SolveOpts(50000, 1e-8, kind, 200, 0)
+            if kind == 1 and self_steps > 0 and k == self_steps:
+                ft_pairs = gpu.lib().sod_gpu_precond_harvest_count(c.h)
+                t0 = time.perf_counter()
+                c.call("sod_gpu_precond_train", ft_steps, ft_batch, ft_lr, 11, C.byref(ft_loss))
+                ft_s = time.perf_counter() - t0
+            o = gpu.SolveOpts(50000, 1e-8, kind, 200, 1 if (kind == 1 and k < self_steps) else 0)
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
             it.append(st.iterations)
             ms.append(st.seconds * 1e3)
@@ -287,7 +299,10 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
                         f"BDF3/EXT3-step pressure systems, FP64-certified tol 1e-8",
             "harvest_steps": harvest_steps, "compare_steps": compare_steps, "harvest_capacity": capacity,
             "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
-            "final_training_loss": round(float(loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],
+            "final_training_loss": round(float(loss.value), 4),
+            "self_harvest_steps": self_steps, "self_harvest_pairs": ft_pairs, "finetune_steps": ft_steps,
+            "finetune_batch": ft_batch, "finetune_lr": ft_lr, "finetune_seconds": round(ft_s, 2),
+            "finetune_loss": round(float(ft_loss.value), 4), "jacobi": res["jacobi"], "learned": res["learned"],
             "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3),
             "speedup_wall_first_100_steps": round(res["jacobi"]["mean_solve_ms_first_100"] /
                                                   res["learned"]["mean_solve_ms_first_100"], 3),
@@ -389,6 +404,9 @@ def main():
     ap.add_argument("--p-compare", type=int, default=800)
     ap.add_argument("--p-train", type=int, default=300)
     ap.add_argument("--p-capacity", type=int, default=256, help="harvested (r, e) pairs kept for training")
+    ap.add_argument("--p-self", type=int, default=16,
+                    help="learned steps that harvest from their own solves before fine-tuning (0: none)")
+    ap.add_argument("--p-finetune", type=int, default=200, help="Adam steps of the fine-tuning")
     ap.add_argument("--precision-study", action="store_true",
                     help="run only the FP32/FP64 precision study against the FP64 oracle (prints its JSON object)")
     ap.add_argument("--ps-nelem1d", type=int, default=16)
@@ -396,7 +414,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     pkw = dict(nelem1d=args.p_nelem1d, harvest_steps=args.p_harvest, compare_steps=args.p_compare,
-               train_steps=args.p_train, capacity=args.p_capacity)
+               train_steps=args.p_train, capacity=args.p_capacity, self_steps=args.p_self, ft_steps=args.p_finetune)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

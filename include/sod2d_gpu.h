@@ -230,6 +230,11 @@ int sod_gpu_precond_loss_grad(sod_gpu_ctx *ctx, const double *r, const double *e
                               float *grad_host);
 /* Number of harvested pairs available for training. */
 int sod_gpu_precond_harvest_count(sod_gpu_ctx *ctx);
+/* Start a new harvest and training phase: drop the harvested pairs and the
+ * Adam moments, keep the parameters.  Solves with precond = 1 and
+ * harvest = 1 then record pairs from the learned map's own iterations,
+ * and sod_gpu_precond_train fine-tunes on them. */
+int sod_gpu_precond_restart_harvest(sod_gpu_ctx *ctx);
 /* Adam: `steps` updates over mini-batches of `batch` (<= 16) harvested
  * pairs; *final_loss (host) = mean loss of the last batch. */
 int sod_gpu_precond_train(sod_gpu_ctx *ctx, int steps, int batch, float lr, uint64_t seed, float *final_loss);

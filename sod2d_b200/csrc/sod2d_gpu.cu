@@ -965,8 +965,10 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
     if (!NT.ready) return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
     if ((rc = ensure_gains(c))) return rc;
   }
-  // harvest snapshots (x_k, r_k) after k = 0..8, 16, 32, ... iterations
-  const bool harvest = opts->harvest && NT.ready && NT.cap > 0 && kind == 0;
+  // harvest snapshots (x_k, r_k) after k = 0..8, 16, 32, ... iterations, from
+  // Jacobi solves (first training) or from solves with the learned map
+  // itself (fine-tuning on the residuals it meets)
+  const bool harvest = opts->harvest && NT.ready && NT.cap > 0;
   struct Snap {
     int slot, si, iter;
     bool fresh;
@@ -1834,6 +1836,17 @@ int sod_gpu_precond_harvest_count(sod_gpu_ctx *c) { return c ? c->net.count : 0;
 
 // Adam on the harvested (r, e) pairs: `steps` updates of `batch` pairs each;
 // *final_loss (host) = mean relative A-norm loss of the last batch.
+int sod_gpu_precond_restart_harvest(sod_gpu_ctx *c) {
+  if (!c || !c->net.ready) return fail(SOD_GPU_EINVAL, "learned preconditioner not set up (sod_gpu_precond_init)");
+  auto &NT = c->net;
+  NT.count = 0;
+  NT.offered = 0;
+  NT.step = 0;
+  CUDA_TRY(cudaMemsetAsync(NT.m1, 0, (size_t)NT.nparam * 4, c->stream));
+  CUDA_TRY(cudaMemsetAsync(NT.m2, 0, (size_t)NT.nparam * 4, c->stream));
+  return c->finish();
+}
+
 int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64_t seed, float *final_loss) {
   if (!c || !c->net.ready || steps < 0 || batch < 1 || batch > 16) return fail(SOD_GPU_EINVAL, "bad argument");
   auto &NT = c->net;

@@ -84,6 +84,7 @@ SIGNATURES = {
     "sod_gpu_precond_apply": (C.c_int, [VP, VP, VP]),
     "sod_gpu_precond_loss_grad": (C.c_int, [VP, VP, VP, C.POINTER(C.c_double), VP]),
     "sod_gpu_precond_harvest_count": (C.c_int, [VP]),
+    "sod_gpu_precond_restart_harvest": (C.c_int, [VP]),
     "sod_gpu_precond_train": (C.c_int, [VP, C.c_int, C.c_int, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "sod_gpu_incomp_init": (C.c_int, [VP, VP, C.c_double]),
     "sod_gpu_incomp_step": (C.c_int, [VP, C.c_float, VP, VP]),

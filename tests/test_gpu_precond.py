@@ -121,3 +121,44 @@ def test_trained_network_beats_jacobi(gpu):
     assert out["learned"][1] < 1e-8 and out["learned"][2] == 0
     assert out["learned"][0] < 0.6 * out["jacobi"][0]
     ctx.close()
+
+
+def test_self_harvest_finetune(gpu):
+    """Pairs harvested from the learned solver's own iterations (after
+    sod_gpu_precond_restart_harvest) fine-tune the map; the fine-tuned map
+    still certifies every solve and needs no more iterations than before."""
+    m = host.periodic_cube(3, 8)
+    N = m.npoin
+    x, y, z = (m.coord[i * N:(i + 1) * N].astype(np.float64) for i in range(3))
+    u = np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),
+                        np.zeros(N)]).astype(np.float32)
+    ctx = gpu.Context(m, gpu.default_phys())
+    ctx.call("sod_gpu_precond_init", 11, 96)
+    du = torch.from_numpy(u).cuda()
+    ctx.call("sod_gpu_incomp_init", gpu.dptr(du), 1.0 / 1600.0)
+    dt = 0.02
+    st = gpu.SolveStats()
+    for k in range(10):
+        ctx.call("sod_gpu_incomp_step", dt, C.byref(gpu.SolveOpts(20000, 1e-8, 0, 100, 1)), C.byref(st))
+    loss = C.c_float()
+    ctx.call("sod_gpu_precond_train", 300, 8, 3e-3, 5, C.byref(loss))
+    with pytest.raises(RuntimeError):  # no context
+        gpu.check(gpu.lib().sod_gpu_precond_restart_harvest(None), "sod_gpu_precond_restart_harvest")
+    ctx.call("sod_gpu_precond_restart_harvest")
+    assert gpu.lib().sod_gpu_precond_harvest_count(ctx.h) == 0
+    its_before = []
+    for k in range(4):
+        ctx.call("sod_gpu_incomp_step", dt, C.byref(gpu.SolveOpts(20000, 1e-8, 1, 200, 1)), C.byref(st))
+        assert st.res_rel < 1e-8 and st.fallback == 0
+        its_before.append(st.iterations)
+    n_pairs = gpu.lib().sod_gpu_precond_harvest_count(ctx.h)
+    assert n_pairs >= 4 * 9  # iterations 0-8 of every learned solve at least
+    ctx.call("sod_gpu_precond_train", 200, 8, 5e-4, 11, C.byref(loss))
+    its_after = []
+    for k in range(4):
+        ctx.call("sod_gpu_incomp_step", dt, C.byref(gpu.SolveOpts(20000, 1e-8, 1, 200, 0)), C.byref(st))
+        assert st.res_rel < 1e-8 and st.fallback == 0
+        its_after.append(st.iterations)
+    print("learned iterations before fine-tuning", its_before, "after", its_after, "pairs", n_pairs)
+    assert np.mean(its_after) <= 1.1 * np.mean(its_before)
+    ctx.close()
