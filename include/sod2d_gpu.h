@@ -310,6 +310,20 @@ int sod_gpu_comp_init_state(sod_gpu_ctx *ctx, const sod_rk_cfg_t *cfg, const flo
                             const float *csound, const float *machno, const float *eta);
 /* One time step of size dt. */
 int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *ctx, float dt);
+/* One step of the IMEX integrator instead of the RK step: imex_main,
+ * src/lib_sod2d/sources/time_integ_imex.f90:181-525, for a periodic case
+ * (no wall model, source terms or LES): explicit convection, implicit
+ * diffusion with the LPS stabilisation of the step's initial state, the
+ * ARK tables of init_imex_solver (time_integ_imex.f90:42-158) for 3 or 4
+ * stages (sod_rk_cfg_t.stages), and per implicit stage conjGrad_imex
+ * (src/lib_sod2d/sources/mod_solver_imex.f90:25-342) with maxIter and tol
+ * (the reference's defaults 200 and 1e-3, TGVCompSolver.f90:90-93); then
+ * the entropy viscosity and Sutherland update of the RK step.  Needs
+ * fp64_state = 0 (the reference's FP32 state). */
+int sod_gpu_comp_imex_step(sod_gpu_ctx *ctx, float dt, int maxIter, double tol);
+/* CG iterations summed over the last IMEX step's stages and the last
+ * stage's ||r||/||r0|| (host). */
+int sod_gpu_comp_imex_stats(sod_gpu_ctx *ctx, int *cg_iters, double *cg_res);
 /* CFL time step (adapt_dt_cfl, src/lib_sod2d/sources/mod_time_ops.f90:11-62),
  * written to *dt (host). */
 int sod_gpu_comp_adapt_dt(sod_gpu_ctx *ctx, float cfl_conv, float cfl_diff, float *dt);

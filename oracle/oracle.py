@@ -39,7 +39,7 @@ class CompParams(C.Structure):
                 ("rho_inf", C.c_double), ("p_inf", C.c_double), ("cfl_conv", C.c_double),
                 ("cfl_diff", C.c_double), ("maxPhysTime", C.c_double), ("stages", C.c_int),
                 ("rk_n", C.c_int), ("lps", C.c_int), ("log_first", C.c_int), ("log_step", C.c_int),
-                ("first_mue", C.c_int)]
+                ("first_mue", C.c_int), ("imex", C.c_int), ("imex_maxiter", C.c_int), ("imex_tol", C.c_double)]
 
 
 def lib() -> C.CDLL:
@@ -116,9 +116,13 @@ class OracleMesh:
 
 
 def comp_params(ic, cfl_conv=0.5, cfl_diff=0.5, stages=5, rk_n=1, lps=True, maxPhysTime=0.0,
-                log_first=1, log_step=10, first_mue=True) -> CompParams:
+                log_first=1, log_step=10, first_mue=True, imex=False, imex_maxiter=200,
+                imex_tol=1e-3) -> CompParams:
+    """imex: the IMEX integrator (imex_main) with `stages` = 3 or 4 and the
+    implicit solve's maxIter / tol (TGVCompSolver.f90:90-93 defaults)."""
     return CompParams(ic.gamma, ic.Rgas, ic.Cp, ic.Prt, ic.rho0, ic.P0, cfl_conv, cfl_diff, maxPhysTime,
-                      stages, rk_n, int(lps), log_first, log_step, int(first_mue))
+                      stages, rk_n, int(lps), log_first, log_step, int(first_mue), int(imex), imex_maxiter,
+                      imex_tol)
 
 
 def tgv_comp_run(om: OracleMesh, ic, prm: CompParams, nsteps: int, max_rows: int = 4096):

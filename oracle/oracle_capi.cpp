@@ -27,6 +27,10 @@ typedef struct {
   // step, the behaviour the CPU regression history
   // Tests/TGV_Compressible/CPU/LS_RK_5/Reference/analysis_cube-4.dat shows.
   int first_mue;
+  // 1: IMEX integrator (imex_main, time_integ_imex.f90) with `stages` (3 or
+  // 4) stages and the implicit solve's maxIter / tol; 0: SSP LS-RK
+  int imex, imex_maxiter;
+  double imex_tol;
 } oracle_comp_params_t;
 
 }  // extern "C"
@@ -93,6 +97,10 @@ struct CompSolver {
   std::vector<R> Rmass, Rener, Rmom, Reta, auxReta, f_eta, aux_h, divU, vorti, tau_stab;
   std::vector<R> PMass, PEner, PMX, PMY, PMZ;
   R lam[7][7], gam[7][7];
+  // IMEX: Butcher tables (1-based) and per-stage explicit / implicit residuals
+  R ae[5][5] = {}, ai[5][5] = {};
+  std::vector<R> RmI, RqI, ReI, DmI, DqI, DeI, Rms, Rqs, Res, Pz;
+  int cg_iters = 0;
   bool first = true;
   R dt = 0;
   double time = 0;
@@ -202,6 +210,141 @@ struct CompSolver {
     sutherland<R>(N, T2, mu_factor.data(), mu_fluid.data());
   }
 
+  // Butcher tables of init_imex_solver, time_integ_imex.f90:42-158
+  int imex_coeffs(int S) {
+    if (S == 4) {
+      const R bi[5] = {0, R(4.0 / 15.0), R(1.0 / 3.0), R(7.0 / 30.0), R(1.0 / 6.0)};
+      const R be[5] = {0, R(1.0 / 4.0), R(0.0), R(3.0 / 4.0), R(0.0)};
+      ai[2][1] = bi[1]; ai[2][2] = bi[1];
+      ai[3][1] = bi[1]; ai[3][2] = bi[2]; ai[3][3] = R(1.0 / 15.0);
+      ai[4][1] = bi[1]; ai[4][2] = bi[2]; ai[4][3] = bi[3]; ai[4][4] = bi[4];
+      ae[2][1] = R(8.0 / 15.0);
+      ae[3][1] = be[1]; ae[3][2] = R(5.0 / 12.0);
+      ae[4][1] = be[1]; ae[4][2] = be[2]; ae[4][3] = be[3]; ae[4][4] = be[4];
+      return 0;
+    }
+    if (S == 3) {
+      ai[2][1] = R(0.353842865099275); ai[2][2] = R(0.353842865099275);
+      ai[3][1] = R(0.398930808264689); ai[3][2] = R(0.345755244189622); ai[3][3] = R(0.255313947545689);
+      ae[2][1] = R(0.711664700366941);
+      ae[3][1] = R(0.077338168947683); ae[3][2] = R(0.917273367886007);
+      return 0;
+    }
+    return -1;
+  }
+
+  // EOS of a stage, time_integ_imex.f90:424-438 (also csound, Mach)
+  void eos2() {
+    const R gm = (R)prm.gamma, Rgas = (R)prm.Rgas;
+    R *rho2 = lv(rho, 2), *u2 = lv(u, 2, 3), *q2 = lv(q, 2, 3), *pr2 = lv(pr, 2), *E2 = lv(E, 2), *T2 = lv(Tem, 2);
+    R *ei2 = lv(e_int, 2);
+    for (int t = 0; t < m.npoin_w; ++t) {
+      long long p = m.lpoin_w[t] - 1;
+      R umag = 0;
+      for (int d = 0; d < 3; ++d) {
+        u2[p + N * d] = q2[p + N * d] / rho2[p];
+        umag = umag + u2[p + N * d] * u2[p + N * d];
+      }
+      ei2[p] = (E2[p] / rho2[p]) - R(0.5) * umag;
+      pr2[p] = rho2[p] * (gm - R(1.0)) * ei2[p];
+      aux_h[p] = (gm / (gm - R(1.0))) * pr2[p] / rho2[p];
+      csound[p] = std::sqrt(gm * pr2[p] / rho2[p]);
+      umag = std::sqrt(umag);
+      machno[p] = umag / csound[p];
+      T2[p] = pr2[p] / (rho2[p] * Rgas);
+    }
+  }
+
+  // imex_main, time_integ_imex.f90:181-525 (periodic, no wall model, source
+  // or LES; flag_use_ducros and flag_total_enthalpy off).  Convection and
+  // diffusion residuals carry the subroutines' default fact +1 (their saved
+  // aux_fact is never set otherwise on this path).  full_stab_ijk (fact -1)
+  // is taken as full_diff_stab_ijk with zero viscosities and fact +1: the
+  // same terms with the sign moved inside, equal in every bit.
+  void imex_step() {
+    const int S = prm.stages;
+    const R gm = (R)prm.gamma;
+    R *u1 = lv(u, 1, 3), *u2 = lv(u, 2, 3), *q1 = lv(q, 1, 3), *q2 = lv(q, 2, 3);
+    R *rho1 = lv(rho, 1), *rho2 = lv(rho, 2), *eta1 = lv(eta, 1), *eta2 = lv(eta, 2);
+    R *E1 = lv(E, 1), *E2 = lv(E, 2), *pr1 = lv(pr, 1), *T1 = lv(Tem, 1);
+    auto st = [&](std::vector<R> &a, int k, int nc = 1) { return a.data() + (size_t)N * nc * (k - 1); };
+    if (first) {
+      first = false;
+      for (int t = 0; t < m.npoin_w; ++t) {
+        long long p = m.lpoin_w[t] - 1;
+        for (int d = 0; d < 3; ++d) f_eta[p + N * d] = u1[p + N * d] * eta1[p];
+      }
+      generic_scalar_convec_ijk<R>(m, g, f_eta.data(), eta1, u1, Reta.data(), true, R(1));
+      lumped_solver<R>(m, g, Reta.data(), 1);
+      smart_visc_spectral_imex<R>(m, g, Reta.data(), rho1, u1, csound.data(), mu_e.data());
+      if (!prm.first_mue) std::fill(mu_e.begin(), mu_e.end(), R(0));
+      for (int t = 0; t < m.npoin_w; ++t) {
+        long long p = m.lpoin_w[t] - 1;
+        aux_h[p] = (gm / (gm - R(1.0))) * pr1[p] / rho1[p];
+      }
+      full_convec_ijk<R>(m, g, u1, q1, rho1, pr1, aux_h.data(), st(RmI, 1), st(RqI, 1, 3), st(ReI, 1), true, R(1));
+      full_diffusion_ijk<R>(m, g, (R)prm.Cp, (R)prm.Prt, rho1, rho1, u1, T1, mu_fluid.data(), mu_e.data(),
+                            mu_sgs.data(), st(DmI, 1), st(DqI, 1, 3), st(DeI, 1), true, R(1));
+    } else {
+      std::copy(st(RmI, S), st(RmI, S) + N, st(RmI, 1));
+      std::copy(st(DmI, S), st(DmI, S) + N, st(DmI, 1));
+      std::copy(st(ReI, S), st(ReI, S) + N, st(ReI, 1));
+      std::copy(st(DeI, S), st(DeI, S) + N, st(DeI, 1));
+      std::copy(st(RqI, S, 3), st(RqI, S, 3) + 3 * N, st(RqI, 1, 3));
+      std::copy(st(DqI, S, 3), st(DqI, S, 3) + 3 * N, st(DqI, 1, 3));
+    }
+    if (prm.lps) {
+      comp_tau<R>(m, g, csound.data(), u2, tau_stab.data());
+      full_proj_ijk<R>(m, g, rho1, u1, T1, PMass.data(), PEner.data(), PMX.data(), PMY.data(), PMZ.data());
+      full_diff_stab_ijk<R>(m, g, (R)prm.Cp, (R)prm.Prt, rho1, rho1, u1, T1, Pz.data(), Pz.data(), Pz.data(),
+                            PMass.data(), PEner.data(), PMX.data(), PMY.data(), PMZ.data(), tau_stab.data(),
+                            Rms.data(), Rqs.data(), Res.data(), true, R(1));
+    }
+    for (int is = 2; is <= S; ++is) {
+      for (long long p = 0; p < N; ++p) {
+        rho2[p] = -dt * Rms[p];
+        E2[p] = -dt * Res[p];
+        for (int d = 0; d < 3; ++d) q2[p + N * d] = -dt * Rqs[p + N * d];
+        for (int js = 1; js < is; ++js) {
+          rho2[p] = rho2[p] - dt * ae[is][js] * st(RmI, js)[p] - dt * ai[is][js] * st(DmI, js)[p];
+          E2[p] = E2[p] - dt * ae[is][js] * st(ReI, js)[p] - dt * ai[is][js] * st(DeI, js)[p];
+          for (int d = 0; d < 3; ++d)
+            q2[p + N * d] = q2[p + N * d] - dt * ae[is][js] * st(RqI, js, 3)[p + N * d] -
+                            dt * ai[is][js] * st(DqI, js, 3)[p + N * d];
+        }
+      }
+      for (long long p = 0; p < N; ++p) {
+        rho2[p] = rho2[p] + rho1[p] * g.Ml[p];
+        E2[p] = E2[p] + E1[p] * g.Ml[p];
+        for (int d = 0; d < 3; ++d) q2[p + N * d] = q2[p + N * d] + q1[p + N * d] * g.Ml[p];
+      }
+      double res = 0.0;
+      cg_iters = conjGrad_imex<R>(m, g, ai[is][is], dt, gm, (R)prm.Rgas, (R)prm.Cp, (R)prm.Prt, mu_fluid.data(),
+                                  mu_e.data(), mu_sgs.data(), rho1, E1, q1, rho2, E2, q2, prm.imex_maxiter,
+                                  prm.imex_tol, &res);
+      eos2();
+      full_convec_ijk<R>(m, g, u2, q2, rho2, lv(pr, 2), aux_h.data(), st(RmI, is), st(RqI, is, 3), st(ReI, is), true,
+                         R(1));
+      full_diffusion_ijk<R>(m, g, (R)prm.Cp, (R)prm.Prt, rho2, rho2, u2, lv(Tem, 2), mu_fluid.data(), mu_e.data(),
+                            mu_sgs.data(), st(DmI, is), st(DqI, is, 3), st(DeI, is), true, R(1));
+    }
+    R *pr2 = lv(pr, 2), *T2 = lv(Tem, 2);
+    thermo_entropy<R>(m, gm, (R)prm.p_inf, (R)prm.rho_inf, rho2, pr2, u1, eta.data(), f_eta.data());
+    R *Reta1 = Reta.data(), *Reta2 = Reta.data() + N;
+    generic_scalar_convec_ijk<R>(m, g, f_eta.data(), eta1, u1, Reta2, true, R(1));
+    lumped_solver<R>(m, g, Reta2, 1);
+    for (int t = 0; t < m.npoin_w; ++t) {
+      long long p = m.lpoin_w[t] - 1;
+      auxReta[p] = (R(1.5) * Reta2[p] - R(0.5) * Reta1[p]) + R(1.0) * (eta2[p] - eta1[p]) / dt;
+      Reta1[p] = Reta2[p];
+    }
+    smart_visc_spectral_imex<R>(m, g, auxReta.data(), rho2, u2, csound.data(), mu_e.data());
+    eval_divergence<R>(m, g, u2, divU.data());
+    compute_vorticity<R>(m, g, u2, vorti.data());
+    ducros_visc_limit<R>(m, g, rho2, u2, divU.data(), vorti.data(), csound.data(), mu_e.data());
+    sutherland<R>(N, T2, mu_factor.data(), mu_fluid.data());
+  }
+
   void analysis(double *row) {
     R *rho2 = lv(rho, 2), *u2 = lv(u, 2, 3);
     double EK = volAvg_EK<R>(m, g, (R)prm.rho_inf, rho2, u2);
@@ -229,7 +372,7 @@ int tgv_comp_run(const oracle_mesh_t *cm, const oracle_comp_params_t *prm, const
   s.prm = *prm;
   s.N = s.m.npoin; s.NE = s.m.nelem; s.n = s.m.nnode;
   const long long N = s.N;
-  if (rk_coeffs<R>(prm->stages, prm->rk_n, s.lam, s.gam)) return -1;
+  if (prm->imex ? s.imex_coeffs(prm->stages) : rk_coeffs<R>(prm->stages, prm->rk_n, s.lam, s.gam)) return -1;
   s.rho.assign(N * 4, 0); s.u.assign(N * 12, 0); s.q.assign(N * 12, 0); s.pr.assign(N * 4, 0); s.E.assign(N * 4, 0);
   s.Tem.assign(N * 2, 0); s.e_int.assign(N * 2, 0); s.eta.assign(N * 4, 0); s.mu_fluid.assign(N, 0);
   s.csound.assign(N, 0); s.machno.assign(N, 0); s.mu_e.assign(s.NE * s.n, 0); s.mu_sgs.assign(s.NE * s.n, 0);
@@ -238,6 +381,12 @@ int tgv_comp_run(const oracle_mesh_t *cm, const oracle_comp_params_t *prm, const
   s.auxReta.assign(N, 0); s.f_eta.assign(N * 3, 0); s.aux_h.assign(N, 0); s.divU.assign(N, 0);
   s.vorti.assign(N * 3, 0); s.tau_stab.assign(s.NE, 0);
   s.PMass.assign(N * 3, 0); s.PEner.assign(N * 3, 0); s.PMX.assign(N * 3, 0); s.PMY.assign(N * 3, 0); s.PMZ.assign(N * 3, 0);
+  if (prm->imex) {
+    const int S = prm->stages;
+    s.RmI.assign(N * S, 0); s.ReI.assign(N * S, 0); s.DmI.assign(N * S, 0); s.DeI.assign(N * S, 0);
+    s.RqI.assign(N * 3 * S, 0); s.DqI.assign(N * 3 * S, 0);
+    s.Rms.assign(N, 0); s.Res.assign(N, 0); s.Rqs.assign(N * 3, 0); s.Pz.assign((size_t)s.NE * s.n + N, 0);
+  }
   // init layout: rho, u(3), q(3), pr, E, Tem, e_int, csound, machno, eta -> 14 N values
   const R *I = init;
   std::copy(I, I + N, s.lv(s.rho, 2)); I += N;
@@ -264,7 +413,8 @@ int tgv_comp_run(const oracle_mesh_t *cm, const oracle_comp_params_t *prm, const
     std::copy(s.lv(s.Tem, 2), s.lv(s.Tem, 2) + N, s.lv(s.Tem, 1));
     std::copy(s.lv(s.e_int, 2), s.lv(s.e_int, 2) + N, s.lv(s.e_int, 1));
     std::copy(s.lv(s.eta, 2), s.lv(s.eta, 2) + N, s.lv(s.eta, 1));
-    s.rk_step();
+    if (prm->imex) s.imex_step();
+    else s.rk_step();
     s.time = (double)((R)s.time + s.dt);
     if (log_next == istep) {
       if (rows < max_rows) s.analysis(hist + 6 * rows++);

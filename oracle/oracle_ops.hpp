@@ -1142,4 +1142,102 @@ int conjGrad_veloc(const Mesh &m, const Geo<R> &g, R fact, R dt, const R *helem_
   return iter > maxIter ? maxIter : iter;
 }
 
+// ---- conjGrad_imex (periodic), src/lib_sod2d/sources/mod_solver_imex.f90:25-342
+// CG on the five conserved variables v = (mass, energy, momentum x, y, z):
+// Ml x + fact dt D(x) = b, where D(v) = full_diffusion_ijk(init, fact 1) with
+// rho_n = the iterate's density x_mass, the argument's density v_mass,
+// velocity v_mom / x_mass and temperature from v_E, v_mom and x_mass
+// (mod_solver_imex.f90:97-107, 310-320); preconditioner Ml / dt; x0 = the
+// state at the start of the step; vectors in R, dots in FP64 (node-major,
+// variable inner), alpha and beta rounded to R.  (rho, E, q): in b, out x
+// on the working nodes.  Returns the iteration count.
+template <class R>
+int conjGrad_imex(const Mesh &m, const Geo<R> &g, R fact, R dt, R gamma, R Rgas, R Cp, R Prt, const R *mu_fluid,
+                  const R *mu_e, const R *mu_sgs, const R *rho0, const R *E0, const R *q0, R *rho, R *E, R *q,
+                  int maxIter, double tol, double *res_rel) {
+  const long long N = m.npoin;
+  constexpr int NV = 5;
+  std::vector<R> x(NV * N, 0), r0(NV * N, 0), p0(NV * N, 0), qn(NV * N, 0), b(NV * N, 0), z0(NV * N, 0),
+      z1(NV * N, 0), au(3 * N, 0), aT(N, 0);
+  auto W = [&](auto f) {
+    for (int t = 0; t < m.npoin_w; ++t) f((long long)m.lpoin_w[t] - 1);
+  };
+  W([&](long long p) {
+    b[p] = rho[p]; x[p] = rho0[p];
+    b[p + N] = E[p]; x[p + N] = E0[p];
+    for (int d = 0; d < 3; ++d) { b[p + N * (2 + d)] = q[p + N * d]; x[p + N * (2 + d)] = q0[p + N * d]; }
+  });
+  // velocity and temperature of the argument v over the iterate's density
+  auto prim = [&](const R *v) {
+    W([&](long long p) {
+      const R rhol = x[p], El = v[p + N];
+      R umag = 0;
+      for (int d = 0; d < 3; ++d) {
+        au[p + N * d] = v[p + N * (2 + d)] / rhol;
+        umag = umag + (au[p + N * d] * au[p + N * d]);
+      }
+      const R e_int_l = (El / rhol) - R(0.5) * umag;
+      aT[p] = rhol * (gamma - R(1.0)) * e_int_l / (rhol * Rgas);
+    });
+  };
+  auto apply = [&](const R *v) {  // qn = v Ml + D(v) fact dt
+    full_diffusion_ijk(m, g, Cp, Prt, x.data(), v, au.data(), aT.data(), mu_fluid, mu_e, mu_sgs, qn.data(),
+                       qn.data() + 2 * N, qn.data() + N, true, R(1));
+    W([&](long long p) {
+      for (int k = 0; k < NV; ++k) qn[p + N * k] = v[p + N * k] * g.Ml[p] + qn[p + N * k] * fact * dt;
+    });
+  };
+  auto dot = [&](auto f) {
+    double s = 0.0;
+    W([&](long long p) {
+      for (int k = 0; k < NV; ++k) s += f(p + N * k);
+    });
+    return s;
+  };
+  prim(x.data());
+  apply(x.data());
+  W([&](long long p) {
+    for (int k = 0; k < NV; ++k) r0[p + N * k] = b[p + N * k] - qn[p + N * k];
+  });
+  W([&](long long p) {
+    const R M = g.Ml[p] / dt;
+    for (int k = 0; k < NV; ++k) { z0[p + N * k] = r0[p + N * k] / M; p0[p + N * k] = z0[p + N * k]; }
+  });
+  prim(p0.data());
+  const double auxB = std::sqrt(dot([&](long long k) { return (double)(r0[k] * r0[k]); }));
+  double nrm = auxB;
+  int iter;
+  for (iter = 1; iter <= maxIter; ++iter) {
+    apply(p0.data());
+    const double Q1 = dot([&](long long k) { return (double)(r0[k] * z0[k]); });
+    const double Q2 = dot([&](long long k) { return (double)(p0[k] * qn[k]); });
+    const R alpha = (R)(Q1 / Q2);
+    W([&](long long p) {
+      for (int k = 0; k < NV; ++k) {
+        x[p + N * k] = x[p + N * k] + alpha * p0[p + N * k];
+        r0[p + N * k] = r0[p + N * k] - alpha * qn[p + N * k];
+      }
+    });
+    W([&](long long p) {
+      const R M = g.Ml[p] / dt;
+      for (int k = 0; k < NV; ++k) { z1[p + N * k] = z0[p + N * k]; z0[p + N * k] = r0[p + N * k] / M; }
+    });
+    nrm = std::sqrt(dot([&](long long k) { return (double)(r0[k] * r0[k]); }));
+    if (nrm < tol * auxB) break;
+    const double T = dot([&](long long k) { return (double)(r0[k] * (z0[k] - z1[k])); });
+    const R beta = (R)(T / Q1);
+    W([&](long long p) {
+      for (int k = 0; k < NV; ++k) p0[p + N * k] = z0[p + N * k] + beta * p0[p + N * k];
+    });
+    prim(p0.data());
+  }
+  W([&](long long p) {
+    rho[p] = x[p];
+    E[p] = x[p + N];
+    for (int d = 0; d < 3; ++d) q[p + N * d] = x[p + N * (2 + d)];
+  });
+  *res_rel = auxB > 0 ? nrm / auxB : 0.0;
+  return iter > maxIter ? maxIter : iter;
+}
+
 }  // namespace oracle

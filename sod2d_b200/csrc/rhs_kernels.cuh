@@ -218,6 +218,8 @@ struct RhsArgs {
   const float *mue_t;     // [nelem][N] tensor order (internal copy of mu_e)
   const float *musgs_t;   // [nelem][N] or null
   const float *tau_stab;  // (nelem)
+  const float *rho_n;     // IN_DIFF: density of the nu_e and mu_sgs terms when it differs
+                          // from rho (full_diffusion_ijk's rho_n); null: rho
   const float *proj12;    // [npoin][12] mass-inverted projections (internal):
                           // tau00 tau01 tau02 tau11 tau12 tau22 gradRho(3) gradT(3)
   float fact_c, fact_d;
@@ -250,7 +252,7 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   const bool active = (e < m.nelem) && (t < N);
   const long long NP = m.npoin;
   NodeQ s;
-  float mu = 0.f;
+  float mu = 0.f, rhon_in = 0.f;
   int node = 0;
   float He[9], gv = 0.f;
   if (active) {
@@ -270,6 +272,7 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
       s.p = A.pr[node]; s.h = A.E[node]; s.T = 0.f;
     } else {
       s.rho = A.rho[node];
+      rhon_in = A.rho_n ? A.rho_n[node] : s.rho;
       s.u0 = A.u[node]; s.u1 = A.u[node + NP]; s.u2 = A.u[node + 2 * NP];
       s.T = A.Tem[node];
       mu = A.mu_fluid[node];
@@ -406,7 +409,7 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
       for (int a = 0; a < 3; ++a) gradT[a] = He[a] * a0 + He[a + 3] * a1 + He[a + 6] * a2;
       const float mue = A.mue_t[e * N + t];
       const float musgs = A.musgs_t ? A.musgs_t[e * N + t] : 0.f;
-      const float rhon = s.rho;
+      const float rhon = IN == IN_DIFF ? rhon_in : s.rho;
       nu_e = ph.c_rho * mue / rhon;
       const float mu_fgp = mu + rhon * musgs;
       const float mu_egp = mue;

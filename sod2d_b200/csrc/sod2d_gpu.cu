@@ -6,6 +6,7 @@
 #include "incomp_kernels.cuh"
 #include "precond_net.cuh"
 #include "veloc_kernels.cuh"
+#include "imex_kernels.cuh"
 
 #include <cuda_runtime.h>
 
@@ -128,6 +129,15 @@ struct sod_gpu_ctx {
     unsigned int *bits;  // [0] min rho, [1] dt, [2] max Mach
     double *sums;        // [3]
   } comp;
+  // IMEX integrator scratch (five-variable blocks [mass][energy][momentum])
+  struct Imex {
+    float *R = nullptr, *D = nullptr;  // [4 stages][5N] explicit / implicit residuals
+    float *stab = nullptr, *lvl1 = nullptr, *aux_h = nullptr;
+    float *x = nullptr, *r = nullptr, *p = nullptr, *qn = nullptr, *b = nullptr, *z = nullptr, *z1 = nullptr;
+    float *au = nullptr, *aT = nullptr, *zmu = nullptr, *zmue = nullptr;  // CG primitives; zero viscosities
+    int cg_iters = 0;
+    double cg_res = 0.0;
+  } imex;
 
   MeshDev md() const {
     MeshDev m;
@@ -488,7 +498,6 @@ int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
   if (!c || !rho_n || !rho || !u || !Tem || !mu_fluid || !mu_e || !ProjMass || !ProjEner || !ProjMX || !ProjMY ||
       !ProjMZ || !tau_stab || !Rmass || !Rmom || !Rener)
     return fail(SOD_GPU_EINVAL, "bad argument");
-  if (rho_n != rho) return fail(SOD_GPU_EINVAL, "rho_n must alias rho (as every reference caller passes)");
   const long long EN = (long long)c->nelem * c->N;
   k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   if (mu_sgs) {
@@ -522,7 +531,6 @@ int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
                                float fact) {
   if (!c || !rho_n || !rho || !u || !Tem || !mu_fluid || !mu_e || !Rmass || !Rmom || !Rener)
     return fail(SOD_GPU_EINVAL, "bad argument");
-  if (rho_n != rho) return fail(SOD_GPU_EINVAL, "rho_n must alias rho (as every reference caller passes)");
   const long long EN = (long long)c->nelem * c->N;
   k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   if (mu_sgs) {
@@ -534,6 +542,7 @@ int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
   }
   RhsArgs A{};
   A.rho = rho; A.u = u; A.Tem = Tem; A.mu_fluid = mu_fluid;
+  A.rho_n = rho_n != rho ? rho_n : nullptr;
   A.mue_t = c->mue_t; A.musgs_t = mu_sgs ? c->musgs_t : nullptr;
   A.fact_d = fact;
   Phys saved = c->ph;
@@ -1419,6 +1428,239 @@ int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *c, float dt) {
   comp_visc(c, S.aux, S.rho32, S.u2, true);
   k_sutherland<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->lpoin_w, S.mu_factor, S.Tem, S.mu_fluid);
   return c->finish();
+}
+
+}  // extern "C"
+
+// ---- IMEX time step (imex_main) ------------------------------------------
+
+namespace {
+
+int ensure_imex(sod_gpu_ctx *c) {
+  auto &X = c->imex;
+  if (X.R) return 0;
+  const size_t N = c->npoin, EN = (size_t)c->nelem * c->N;
+  int rc;
+  if ((rc = c->alloc(&X.R, 4 * 5 * N)) || (rc = c->alloc(&X.D, 4 * 5 * N)) || (rc = c->alloc(&X.stab, 5 * N)) ||
+      (rc = c->alloc(&X.lvl1, 5 * N)) || (rc = c->alloc(&X.aux_h, N)) || (rc = c->alloc(&X.x, 5 * N)) ||
+      (rc = c->alloc(&X.r, 5 * N)) || (rc = c->alloc(&X.p, 5 * N)) || (rc = c->alloc(&X.qn, 5 * N)) ||
+      (rc = c->alloc(&X.b, 5 * N)) || (rc = c->alloc(&X.z, 5 * N)) || (rc = c->alloc(&X.z1, 5 * N)) ||
+      (rc = c->alloc(&X.au, 3 * N)) || (rc = c->alloc(&X.aT, N)) || (rc = c->alloc(&X.zmu, N)) ||
+      (rc = c->alloc(&X.zmue, EN)))
+    return rc;
+  if (!c->cg.part && ((rc = c->alloc(&c->cg.part, 8 * DOT_BLOCKS)) || (rc = c->alloc(&c->cg.dots, 16)))) return rc;
+  for (float *v : {X.R, X.D}) CUDA_TRY(cudaMemsetAsync(v, 0, 4 * 5 * N * 4, c->stream));
+  for (float *v : {X.stab, X.x, X.r, X.p, X.qn, X.b, X.z, X.z1}) CUDA_TRY(cudaMemsetAsync(v, 0, 5 * N * 4, c->stream));
+  CUDA_TRY(cudaMemsetAsync(X.au, 0, 3 * N * 4, c->stream));
+  for (float *v : {X.aT, X.zmu, X.aux_h}) CUDA_TRY(cudaMemsetAsync(v, 0, N * 4, c->stream));
+  CUDA_TRY(cudaMemsetAsync(X.zmue, 0, EN * 4, c->stream));
+  return 0;
+}
+
+// Butcher tables of init_imex_solver, time_integ_imex.f90:42-158, rounded
+// to FP32 as the reference's real(rp) constants
+ImexCoef imex_coef(int S) {
+  ImexCoef k{};
+  if (S == 4) {
+    const float bi1 = 4.0f / 15.0f, bi2 = 1.0f / 3.0f, bi3 = 7.0f / 30.0f, bi4 = 1.0f / 6.0f;
+    const float be1 = 1.0f / 4.0f, be2 = 0.0f, be3 = 3.0f / 4.0f, be4 = 0.0f;
+    k.ai[2][1] = bi1; k.ai[2][2] = bi1;
+    k.ai[3][1] = bi1; k.ai[3][2] = bi2; k.ai[3][3] = 1.0f / 15.0f;
+    k.ai[4][1] = bi1; k.ai[4][2] = bi2; k.ai[4][3] = bi3; k.ai[4][4] = bi4;
+    k.ae[2][1] = 8.0f / 15.0f;
+    k.ae[3][1] = be1; k.ae[3][2] = 5.0f / 12.0f;
+    k.ae[4][1] = be1; k.ae[4][2] = be2; k.ae[4][3] = be3; k.ae[4][4] = be4;
+  } else {
+    k.ai[2][1] = (float)0.353842865099275; k.ai[2][2] = (float)0.353842865099275;
+    k.ai[3][1] = (float)0.398930808264689; k.ai[3][2] = (float)0.345755244189622;
+    k.ai[3][3] = (float)0.255313947545689;
+    k.ae[2][1] = (float)0.711664700366941;
+    k.ae[3][1] = (float)0.077338168947683; k.ae[3][2] = (float)0.917273367886007;
+  }
+  return k;
+}
+
+// explicit convection (fact +1) of a stage state into a five-variable block
+void imex_convec(sod_gpu_ctx *c, const float *rho, const float *u, const float *q, const float *pr, const float *h,
+                 float *out) {
+  RhsArgs A{};
+  A.rho = rho; A.u = u; A.q = q; A.pr = pr; A.E = h; A.fact_c = 1.0f;
+  dispatch(c, [&](auto L) {
+    L.template rhs<MODE_CONV, IN_PRIM>(c, A);
+    return 0;
+  });
+  const long long N = c->npoin;
+  gather_res(c, out, out + 2 * N, out + N, 0, 0);
+}
+
+// diffusion without LPS (fact +1) into a five-variable block; rho_n null: rho
+void imex_diffusion(sod_gpu_ctx *c, const float *rho_n, const float *rho, const float *u, const float *Tem,
+                    float *out) {
+  auto &S = c->comp;
+  RhsArgs A{};
+  A.rho = rho; A.rho_n = rho_n; A.u = u; A.Tem = Tem; A.mu_fluid = S.mu_fluid; A.mue_t = c->mue_t;
+  A.musgs_t = nullptr; A.fact_d = 1.0f;
+  dispatch(c, [&](auto L) {
+    L.template rhs<MODE_DIFF | MODE_NOLPS, IN_DIFF>(c, A);
+    return 0;
+  });
+  const long long N = c->npoin;
+  gather_res(c, out, out + 2 * N, out + N, 0, 0);
+}
+
+// FP64 sum over the working nodes and the five variables of a (b - c)
+double imex_dot(sod_gpu_ctx *c, const float *a, const float *b, const float *cc, int *rc) {
+  const long long N = c->npoin;
+  DotArgs<float, 5> A{};
+  for (int k = 0; k < 5; ++k) {
+    A.a[k] = a + N * k; A.b[k] = b + N * k; A.c[k] = cc ? cc + N * k : nullptr;
+  }
+  dots<float, 5>(c, A, c->cg.dots + 8);
+  double t[5] = {0, 0, 0, 0, 0};
+  if (cudaMemcpyAsync(t, c->cg.dots + 8, 40, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    *rc = fail(SOD_GPU_ECUDA, "dot product of the IMEX solve failed");
+    return 0.0;
+  }
+  return (((t[0] + t[1]) + t[2]) + t[3]) + t[4];
+}
+
+// conjGrad_imex, mod_solver_imex.f90:25-342 (periodic): x0 = the step's
+// initial state (X.lvl1), right-hand side the stage state in (rho32, E32,
+// q32), which receives the solution on the working nodes.
+int imex_cg(sod_gpu_ctx *c, float fact, float dt, int maxIter, double tol) {
+  auto &S = c->comp;
+  auto &X = c->imex;
+  const long long N = c->npoin;
+  const int nw = c->npoin_w;
+  const unsigned nb = nblk(nw, 256);
+  const float gm1 = c->phys.gamma_gas - 1.0f;
+  CUDA_TRY(cudaMemcpyAsync(X.x, X.lvl1, 5 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(X.b, S.rho32, N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(X.b + N, S.E32, N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(X.b + 2 * N, S.q32, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  auto apply = [&](const float *v) {  // qn = v Ml + fact dt D(v)
+    k_imex_prim<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, gm1, c->phys.Rgas, X.x, v, X.au, X.aT);
+    imex_diffusion(c, X.x, v, X.au, X.aT, X.qn);
+    k_imex_op<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, v, fact, dt, X.qn);
+  };
+  int rc = 0;
+  apply(X.x);
+  k_imex_vec<<<nb, 256, 0, c->stream>>>(0, nw, N, c->lpoin_w, c->Ml, dt, 0.f, 0.f, X.b, X.x, X.r, X.p, X.qn, X.z,
+                                        X.z1);
+  const double auxB = std::sqrt(imex_dot(c, X.r, X.r, nullptr, &rc));
+  if (rc) return rc;
+  double nrm = auxB;
+  int it;
+  for (it = 1; it <= maxIter; ++it) {
+    apply(X.p);
+    const double Q1 = imex_dot(c, X.r, X.z, nullptr, &rc);
+    const double Q2 = imex_dot(c, X.p, X.qn, nullptr, &rc);
+    if (rc) return rc;
+    const float alpha = (float)(Q1 / Q2);
+    k_imex_vec<<<nb, 256, 0, c->stream>>>(1, nw, N, c->lpoin_w, c->Ml, dt, alpha, 0.f, X.b, X.x, X.r, X.p, X.qn,
+                                          X.z, X.z1);
+    nrm = std::sqrt(imex_dot(c, X.r, X.r, nullptr, &rc));
+    if (rc) return rc;
+    if (!std::isfinite(nrm)) return fail(SOD_GPU_ENONFINITE, "non-finite residual in the IMEX solve");
+    if (nrm < tol * auxB) break;
+    const double T = imex_dot(c, X.r, X.z, X.z1, &rc);
+    if (rc) return rc;
+    const float beta = (float)(T / Q1);
+    k_imex_vec<<<nb, 256, 0, c->stream>>>(2, nw, N, c->lpoin_w, c->Ml, dt, 0.f, beta, X.b, X.x, X.r, X.p, X.qn,
+                                          X.z, X.z1);
+  }
+  k_imex_out<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, X.x, S.rho32, S.E32, S.q32);
+  X.cg_iters = it > maxIter ? maxIter : it;
+  X.cg_res = auxB > 0 ? nrm / auxB : 0.0;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sod_gpu_comp_imex_step(sod_gpu_ctx *c, float dt, int maxIter, double tol) {
+  if (!c || !c->comp.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
+  if (!(dt > 0.f) || maxIter < 1 || !(tol > 0.0)) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &S = c->comp;
+  if (S.stages != 3 && S.stages != 4) return fail(SOD_GPU_EINVAL, "the IMEX integrator has 3 or 4 stages");
+  if (S.fp64) return fail(SOD_GPU_EINVAL, "the IMEX integrator runs on the FP32 state (fp64_state = 0)");
+  int rc;
+  if ((rc = ensure_imex(c))) return rc;
+  auto &X = c->imex;
+  const cudaStream_t st = c->stream;
+  const long long N = c->npoin;
+  const int nw = c->npoin_w;
+  const unsigned nb = nblk(nw, 256);
+  const float gm = c->phys.gamma_gas;
+  const ImexCoef K = imex_coef(S.stages);
+  const bool was_async = c->async;
+  c->async = true;
+  // level 1 <- level 2 (CFDSolverBase.f90:1951-1960)
+  CUDA_TRY(cudaMemcpyAsync(S.u1, S.u2, 3 * N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.eta1, S.eta2, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(X.lvl1, S.rho32, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(X.lvl1 + N, S.E32, N * 4, cudaMemcpyDeviceToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(X.lvl1 + 2 * N, S.q32, 3 * N * 4, cudaMemcpyDeviceToDevice, st));
+  const long long B = 5 * N;
+  if (S.first) {  // time_integ_imex.f90:240-273
+    S.first = false;
+    k_feta<<<nb, 256, 0, st>>>(nw, N, c->lpoin_w, S.u1, S.eta1, S.feta);
+    comp_entropy_pass(c, S.Reta1, false);
+    comp_visc(c, S.Reta1, S.rho32, S.u1, false);
+    k_aux_h<<<nb, 256, 0, st>>>(nw, c->lpoin_w, gm / (gm - 1.0f), S.rho32, S.pr, X.aux_h);
+    imex_convec(c, S.rho32, S.u2, S.q32, S.pr, X.aux_h, X.R);
+    imex_diffusion(c, nullptr, S.rho32, S.u2, S.Tem, X.D);
+  } else {  // the last stage's residuals open the step
+    CUDA_TRY(cudaMemcpyAsync(X.R, X.R + (S.stages - 1) * B, B * 4, cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(X.D, X.D + (S.stages - 1) * B, B * 4, cudaMemcpyDeviceToDevice, st));
+  }
+  // LPS stabilisation of the step's initial state (comp_tau, full_proj_ijk,
+  // full_stab_ijk with fact -1 = the LPS part of full_diff_stab_ijk with zero
+  // viscosities and fact +1)
+  k_comp_tau<<<nblk(c->nelem, 8), 256, 0, st>>>(c->nelem, c->N, c->conn, c->helem, S.csound, S.u2, c->npoin,
+                                                c->phys.c_species_stab / (float)c->P, S.tau);
+  {
+    RhsArgs A{};
+    A.rho = S.rho32; A.u = S.u2; A.Tem = S.Tem; A.mu_fluid = X.zmu; A.mue_t = X.zmue; A.musgs_t = nullptr;
+    A.tau_stab = S.tau; A.proj12 = c->proj12; A.fact_d = 1.0f;
+    dispatch(c, [&](auto L) {
+      L.proj(c, true, S.rho32, S.u2, S.Tem);
+      gather_proj_aos(c);
+      L.template rhs<MODE_DIFF, IN_DIFF>(c, A);
+      return 0;
+    });
+    gather_res(c, X.stab, X.stab + 2 * N, X.stab + N, 0, 0);
+  }
+  int iters = 0;
+  for (int is = 2; is <= S.stages; ++is) {
+    k_imex_comb<<<nblk(N, 256), 256, 0, st>>>(N, is, K, dt, c->Ml, X.R, X.D, X.stab, X.lvl1, S.rho32, S.E32, S.q32);
+    if ((rc = imex_cg(c, K.ai[is][is], dt, maxIter, tol))) { c->async = was_async; return rc; }
+    iters += X.cg_iters;
+    k_eos_end<<<nb, 256, 0, st>>>(nw, N, c->lpoin_w, gm - 1.0f, gm, c->phys.Rgas, S.rho32, S.q32, S.E32, S.u2, S.eint,
+                                  S.pr, S.csound, S.machno, S.Tem);
+    k_aux_h<<<nb, 256, 0, st>>>(nw, c->lpoin_w, gm / (gm - 1.0f), S.rho32, S.pr, X.aux_h);
+    imex_convec(c, S.rho32, S.u2, S.q32, S.pr, X.aux_h, X.R + (is - 1) * B);
+    imex_diffusion(c, nullptr, S.rho32, S.u2, S.Tem, X.D + (is - 1) * B);
+  }
+  X.cg_iters = iters;
+  // entropy viscosity of the new state (time_integ_imex.f90:454-505)
+  k_thermo_entropy<<<nb, 256, 0, st>>>(nw, N, c->lpoin_w, gm, c->phys.p_inf, c->phys.rho_inf, S.rho32, S.pr, S.u1,
+                                       S.eta1, S.eta2, S.feta);
+  comp_entropy_pass(c, S.Reta2, true);
+  k_aux_reta<<<nb, 256, 0, st>>>(nw, c->lpoin_w, dt, S.Reta1, S.Reta2, S.eta1, S.eta2, S.aux);
+  comp_visc(c, S.aux, S.rho32, S.u2, true);
+  k_sutherland<<<nb, 256, 0, st>>>(nw, c->lpoin_w, S.mu_factor, S.Tem, S.mu_fluid);
+  c->async = was_async;
+  return c->finish();
+}
+
+int sod_gpu_comp_imex_stats(sod_gpu_ctx *c, int *cg_iters, double *cg_res) {
+  if (!c || !c->comp.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
+  if (cg_iters) *cg_iters = c->imex.cg_iters;
+  if (cg_res) *cg_res = c->imex.cg_res;
+  return 0;
 }
 
 int sod_gpu_comp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float cfl_diff, float *dt) {

@@ -65,6 +65,8 @@ SIGNATURES = {
     "sod_gpu_set_mu_e": (C.c_int, [VP, VP]),
     "sod_gpu_comp_init_state": (C.c_int, [VP, C.POINTER(RkCfg)] + [VP] * 9),
     "sod_gpu_comp_rk_ls_step": (C.c_int, [VP, C.c_float]),
+    "sod_gpu_comp_imex_step": (C.c_int, [VP, C.c_float, C.c_int, C.c_double]),
+    "sod_gpu_comp_imex_stats": (C.c_int, [VP, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "sod_gpu_comp_adapt_dt": (C.c_int, [VP, C.c_float, C.c_float, C.POINTER(C.c_float)]),
     "sod_gpu_comp_analysis": (C.c_int, [VP, C.c_float, C.POINTER(C.c_double)]),
     "sod_gpu_comp_get_state": (C.c_int, [VP] + [VP] * 4),
@@ -189,14 +191,17 @@ class CompSolver:
     """Compressible periodic time loop on the GPU through the C-ABI: the
     driver logic of CFDSolverBase_evalTimeIteration
     (src/lib_mainBaseClass/sources/CFDSolverBase.f90:1929-2164) around
-    sod_gpu_comp_rk_ls_step."""
+    sod_gpu_comp_rk_ls_step, or sod_gpu_comp_imex_step when imex is set
+    (time_integ_imex.f90; the implicit solve's maxIter / tol)."""
 
-    def __init__(self, mesh, ic, stages=4, rk_n=1, fp64_state=True, cfl_conv=0.5, cfl_diff=0.5):
+    def __init__(self, mesh, ic, stages=4, rk_n=1, fp64_state=True, cfl_conv=0.5, cfl_diff=0.5, imex=False,
+                 imex_maxiter=200, imex_tol=1e-3):
         import torch
         self.torch = torch
         self.ctx = Context(mesh, phys_from_ic(ic))
         self.mesh, self.ic = mesh, ic
         self.cfl = (cfl_conv, cfl_diff)
+        self.imex = (imex_maxiter, imex_tol) if imex else None
         dv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
         self._init = [dv(a) for a in (ic.rho, ic.u, ic.q, ic.pr, ic.E, ic.Tem, ic.csound, ic.machno, ic.eta)]
         cfg = RkCfg(stages, rk_n, int(fp64_state), ic.mu_factor)
@@ -215,7 +220,10 @@ class CompSolver:
         return [float(self.time)] + list(out)
 
     def step(self):
-        self.ctx.call("sod_gpu_comp_rk_ls_step", float(self.dt))
+        if self.imex:
+            self.ctx.call("sod_gpu_comp_imex_step", float(self.dt), self.imex[0], self.imex[1])
+        else:
+            self.ctx.call("sod_gpu_comp_rk_ls_step", float(self.dt))
         self.time = np.float32(self.time + np.float32(self.dt))
 
     def run(self, nsteps, log_first=1, log_step=10, max_time=None):

@@ -15,7 +15,8 @@ from pathlib import Path
 SOURCES = {
     "tgv_comp_cpu_lsrk5_8x8x8_p4.dat": "Tests/TGV_Compressible/CPU/LS_RK_5/Reference/analysis_cube-4.dat",
     "tgv_comp_gpu_lsrk5_12x12x12_p4.dat": "Tests/TGV_Compressible/GPU/LS_RK_5/Reference/analysis_cube-1.dat",
-    "tgv_incomp_cpu_ab_12x12x12_p4.dat": "Tests/TGV_Incomp/CPU/AB/Reference/analysis_cube-4.dat",
+    "tgv_comp_cpu_imex4_8x8x8_p4.dat": "Tests/TGV_Compressible/CPU/IMEX/Reference/analysis_cube-4.dat",
+    "tgv_incomp_cpu_ab_8x8x8_p4.dat": "Tests/TGV_Incomp/CPU/AB/Reference/analysis_cube-4.dat",
     "tgv_incomp_gpu_ab_12x12x12_p4.dat": "Tests/TGV_Incomp/GPU/AB/Reference/analysis_cube-1.dat",
 }
 

@@ -70,3 +70,54 @@ def test_fp64_state_close_to_fp32(gpu):
     hb = b.run(10)
     b.close()
     assert rel(hb, ha).max() < 1e-4
+
+
+@pytest.mark.parametrize("stages", [4, 3])
+def test_imex_history_matches_oracle(gpu, stages):
+    """IMEX integrator (imex_main with conjGrad_imex) on the reference's
+    IMEX test case (8^3 order-4 cube, Ma = 1.25, CFL 0.95): the GPU
+    analysis rows agree with the oracle's to 1e-4 relative, the final
+    conserved fields to 1e-5 relative L2; with stages = 4 the first step's
+    time is the reference history's."""
+    m = host.periodic_cube(4, 8)
+    ic = host.tgv_comp_init(m, Ma=1.25)
+    om = O.OracleMesh(m)
+    nsteps = 21
+    prm = O.comp_params(ic, cfl_conv=0.95, cfl_diff=1000.5, stages=stages, imex=True, first_mue=True)
+    ref_hist, ref_fin = O.tgv_comp_run(om, ic, prm, nsteps)
+    s = gpu.CompSolver(m, ic, stages=stages, fp64_state=False, cfl_conv=0.95, cfl_diff=1000.5, imex=True)
+    hist = s.run(nsteps)
+    fin = s.state()
+    its, res = gpu.C.c_int(), gpu.C.c_double()
+    s.ctx.call("sod_gpu_comp_imex_stats", gpu.C.byref(its), gpu.C.byref(res))
+    s.close()
+    assert hist.shape == ref_hist.shape
+    r = rel(hist, ref_hist)
+    print("IMEX stages", stages, "max rel per column:", r.max(0), "CG iterations of the last step", its.value,
+          "residual", res.value)
+    assert r.max() < 1e-4
+    w = m.lpoin_w - 1
+    for k in ("rho", "E"):
+        assert rel_l2(fin[k][w], ref_fin[k][w]) < 1e-5, k
+    assert its.value >= stages - 1 and res.value < 1e-3
+    if stages == 4:
+        gold = O.load_history(GOLD / "tgv_comp_cpu_imex4_8x8x8_p4.dat")
+        assert abs(hist[1, 0] - gold[1, 0]) / gold[1, 0] < 1e-6
+
+
+def test_imex_arguments(gpu):
+    m = host.periodic_cube(3, 2)
+    ic = host.tgv_comp_init(m, Ma=0.1)
+    s = gpu.CompSolver(m, ic, stages=5, fp64_state=False)
+    with pytest.raises(RuntimeError):  # five stages: no IMEX table
+        s.ctx.call("sod_gpu_comp_imex_step", 1e-3, 200, 1e-3)
+    s.close()
+    s = gpu.CompSolver(m, ic, stages=4, fp64_state=True)
+    with pytest.raises(RuntimeError):  # FP64 state
+        s.ctx.call("sod_gpu_comp_imex_step", 1e-3, 200, 1e-3)
+    s.close()
+    s = gpu.CompSolver(m, ic, stages=4, fp64_state=False)
+    for args in ((0.0, 200, 1e-3), (1e-3, 0, 1e-3), (1e-3, 200, 0.0)):
+        with pytest.raises(RuntimeError):
+            s.ctx.call("sod_gpu_comp_imex_step", *args)
+    s.close()

@@ -94,3 +94,42 @@ def test_history_cpu_golden_documented_gap(case8):
     assert k == len(ref)
     assert np.max(np.abs(hist[:k, 1] - ref[:k, 1]) / ref[:k, 1]) < 0.03
     assert np.max(np.abs(hist[:k, 0] - ref[:k, 0]) / np.maximum(ref[:k, 0], 1e-3)) < 0.03
+
+
+def imex_params(ic, **kw):
+    """The reference's IMEX test case: 4 stages, CFL 0.95 (convective only),
+    implicit solve maxIter 200, tol 1e-3
+    (Tests/TGV_Compressible/CPU/IMEX/TGVCompSolver.json)."""
+    return O.comp_params(ic, cfl_conv=0.95, cfl_diff=1000.5, stages=4, imex=True, imex_maxiter=200, imex_tol=1e-3,
+                         **kw)
+
+
+def test_imex_first_step_cpu_golden(case8):
+    """One IMEX step (ARK4 tables, explicit convection, implicit diffusion
+    through conjGrad_imex, LPS stabilisation of the initial state): the t=0
+    row, the time, EK, eps_D and max Mach after step 1 reproduce the CPU
+    IMEX history to its printed precision.  As for the RK history, the file
+    shows no entropy viscosity during the first step (first_mue=False), and
+    eps_S (end-of-step viscosity) carries the start-up gap documented
+    below."""
+    m, ic, om = case8
+    ref = O.load_history(GOLD / "tgv_comp_cpu_imex4_8x8x8_p4.dat")
+    hist, _ = O.tgv_comp_run(om, ic, imex_params(ic, first_mue=False), 1)
+    assert rel(hist[0], ref[0]).max() < 2e-6
+    r = rel(hist[1], ref[1])
+    print("IMEX step 1 rel:", r)
+    assert r[0] < 1e-6 and r[1] < 1e-6 and r[3] < 1e-4 and r[5] < 1e-6
+
+
+@pytest.mark.xfail(strict=False, reason="entropy-viscosity start-up of the reference histories differs "
+                                        "from the restated source (as for the RK history)")
+def test_imex_history_cpu_golden_documented_gap(case8):
+    """Full IMEX history (t <= 5): time within 3% of the CPU file, EK within
+    the gap the end-of-step-1 entropy viscosity opens (measured 9-16%)."""
+    m, ic, om = case8
+    ref = O.load_history(GOLD / "tgv_comp_cpu_imex4_8x8x8_p4.dat")
+    hist, _ = O.tgv_comp_run(om, ic, imex_params(ic, first_mue=False, maxPhysTime=5.0), 1000)
+    k = min(len(hist), len(ref))
+    assert k == len(ref)
+    assert np.max(np.abs(hist[:k, 0] - ref[:k, 0]) / np.maximum(ref[:k, 0], 1e-3)) < 0.03
+    assert np.max(np.abs(hist[:k, 1] - ref[:k, 1]) / ref[:k, 1]) < 0.03
