@@ -337,6 +337,39 @@ def time_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3):
             "Mnode_stages_per_s": round(m.npoin_w * stages / (ms / 1e3) / 1e6, 2), "steps_timed": steps}
 
 
+def imex_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3, Ma=1.25, cfl=0.95):
+    """IMEX time steps (sod_gpu_comp_imex_step: explicit convection, implicit
+    diffusion through conjGrad_imex per stage, LPS of the step's initial
+    state, entropy viscosity) on the Taylor-Green state of a periodic cube
+    nelem1d^3 HEX64 with the reference's IMEX test settings (Ma 1.25, CFL
+    0.95 convective, 4 stages, maxIter 200, tol 1e-3), FP32 state."""
+    import ctypes as C
+    import torch
+    from sod2d_b200 import gpu, host
+    m = host.periodic_cube(PORDER, nelem1d)
+    ic = host.tgv_comp_init(m, Ma=Ma)
+    sv = gpu.CompSolver(m, ic, stages=stages, fp64_state=False, cfl_conv=cfl, cfl_diff=1000.5, imex=True)
+    for _ in range(warmup):
+        sv.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    its, res, cg = C.c_int(), C.c_double(), []
+    e0.record()
+    for _ in range(steps):
+        sv.step()
+        sv.ctx.call("sod_gpu_comp_imex_stats", C.byref(its), C.byref(res))
+        cg.append(its.value)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    sv.close()
+    return {"workload": f"compressible TGV IMEX step, periodic cube {nelem1d}^3 HEX64 (p=3), Ma={Ma}, CFL {cfl}, "
+                        f"{stages}-stage ARK, FP32 state, implicit diffusion CG tol 1e-3, entropy viscosity + LPS",
+            "ms_per_step": round(ms, 4), "stages": stages, "dt": round(float(sv.dt), 6),
+            "cg_iterations_per_step": round(float(np.mean(cg)), 2),
+            "Mnode_stages_per_s": round(m.npoin_w * stages / (ms / 1e3) / 1e6, 2), "steps_timed": steps}
+
+
 def precision_study(nelem1d=16, nsteps=200, porder=3, Ma=0.1, stages=4):
     """Compressible TGV (periodic cube nelem1d^3, order porder, Ma, SSP RK
     with `stages` stages, CFL 0.5, LPS and entropy viscosity on) run three
@@ -568,6 +601,7 @@ def main():
     ctx.close()
     if rank == 0 and world == 1 and not args.no_pressure:
         line["time_step"] = time_step_leg(args.nelem1d)
+        line["imex_step"] = imex_step_leg(args.nelem1d)
         line["pressure_solve"] = pressure_leg(**pkw)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = CpuBaseline().sample()
