@@ -295,12 +295,16 @@ class IncompState:
         self.iltime = 1
 
 
-def bdfext3_step(om, om64, st: IncompState, dt, nu, maxIter=20, tol=1e-4):
+def bdfext3_step(om, om64, st: IncompState, dt, nu, maxIter=20, tol=1e-4, pressure="fp64", p_maxIter=20,
+                 p_tol=1e-2, diag=None):
     """One bdfext3_main_incomp step (periodic mesh, no wall model, source term
     or LES; rho = 1, mu_fluid = nu), time_integ_incomp.f90:88-433, composed
-    of the oracle operators above; the pressure system is solved in FP64 to a
-    1e-12 residual.  Updates st in place and returns the velocity solve's
-    (iterations, ||r||/||r0||)."""
+    of the oracle operators above.  pressure="fp64": the pressure system is
+    solved in FP64 to a 1e-11 residual; pressure="reference": the FP32
+    right-hand side -gamma0 div(u)/dt and conjGrad_pressure_incomp with
+    p_maxIter / p_tol from the previous pressure (diag: its Jacobi
+    diagonal), as the reference runs.  Updates st in place and returns the
+    velocity solve's (iterations, ||r||/||r0||)."""
     N = om.mesh.npoin
     w = om.mesh.lpoin_w - 1
     f32 = np.float32
@@ -320,8 +324,12 @@ def bdfext3_step(om, om64, st: IncompState, dt, nu, maxIter=20, tol=1e-4):
     e = b[0] * Rm2[W] + b[1] * st.Rm1[W] + b[2] * st.Rm3[W]
     u2[W] = (dt * (-e) / Ml[W] + a[0] * st.u1[W] + a[1] * st.u3[W] + a[2] * st.u4[W]) / g0
     st.Rm3, st.Rm1 = st.Rm1, Rm2
-    rhs = -np.float64(g0) * divergence(om, u2).astype(np.float64) / np.float64(dt)
-    p = _pressure_fp64(om64, rhs, st.p)
+    if pressure == "reference":
+        rhs = (f32(-g0) * divergence(om, u2)) / dt
+        p, _, _ = cg_pressure(om, diag, np.asarray(st.p, f32), rhs.astype(f32), maxIter=p_maxIter, tol=p_tol)
+    else:
+        rhs = -np.float64(g0) * divergence(om, u2).astype(np.float64) / np.float64(dt)
+        p = _pressure_fp64(om64, rhs, st.p)
     gp = gradient(om, p.astype(f32))
     u2[W] = (u2[W] - dt * gp[W] / g0) * Ml[W]
     mu = np.full(N, nu, f32)
@@ -331,6 +339,75 @@ def bdfext3_step(om, om64, st: IncompState, dt, nu, maxIter=20, tol=1e-4):
     st.p = p
     st.iltime += 1
     return vit, vres
+
+
+def adapt_dt(om, u, csound, cfl_conv, cfl_diff=1e30, mu_fluid=None, mu_sgs=None, mu_e=None, rho=None):
+    """adapt_dt_cfl, mod_time_ops.f90:7-48; without viscosities (the
+    incompressible solvers' call) only the convective limit acts."""
+    N, EN = om.mesh.npoin, om.mesh.nelem * om.mesh.nnode
+    c = lambda a, n: np.ascontiguousarray(np.zeros(n) if a is None else a, om.dtype)
+    keep = [c(u, 3 * N), c(csound, N), c(mu_fluid, N), c(mu_sgs, EN), c(mu_e, EN),
+            c(np.ones(N) if rho is None else rho, N)]
+    out = C.c_double()
+    om.fn("dt")(C.byref(om.s), _p(keep[0]), _p(keep[1]), float(cfl_conv), float(cfl_diff), _p(keep[2]), _p(keep[3]),
+                _p(keep[4]), _p(keep[5]), C.byref(out))
+    return om.dtype.type(out.value)
+
+
+def analysis(om, rho0, rho, u, mu_fluid, mu_e=None):
+    """volAvg_EK and visc_dissipationRate, mod_analysis.f90:10-144:
+    (EK, eps_S, eps_D, eps_T)."""
+    N, EN = om.mesh.npoin, om.mesh.nelem * om.mesh.nnode
+    c = lambda a, n: np.ascontiguousarray(np.zeros(n) if a is None else a, om.dtype)
+    keep = [c(rho, N), c(u, 3 * N), c(mu_fluid, N), c(mu_e, EN)]
+    out = np.zeros(4)
+    om.fn("analysis")(C.byref(om.s), float(rho0), *(_p(a) for a in keep), _p(out))
+    return out
+
+
+def tgv_incomp_run(om, nsteps, Re=1600.0, cfl_conv=0.5, maxIter=20, tol=1e-2, log_first=1, log_step=10,
+                   max_time=None):
+    """Incompressible Taylor-Green time loop as the reference runs it
+    (TGVSolverIncomp.f90:103-174 initial state, CFDSolverPeriodicIncomp
+    evalDt :119-128 (convective CFL, zero sound speed), bdfext3_main_incomp
+    with conjGrad_pressure_incomp and conjGrad_veloc_incomp sharing maxIter
+    / tol): rows (time, EK, eps_S, eps_D, eps_T, 0) at t = 0, after step
+    log_first and every log_step steps."""
+    f32 = np.float32
+    m = om.mesh
+    N = m.npoin
+    X = m.coord.reshape(3, N).astype(f32)
+    x, y, z = X
+    u0 = np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),
+                         np.zeros(N, f32)]).astype(f32)
+    p0 = (f32(1.0 / 16.0) * (np.cos(f32(2) * x) + np.cos(f32(2) * y)) * (np.cos(f32(2) * z) + f32(2))).astype(f32)
+    nu = f32(1.0) / f32(Re)
+    mu = np.full(N, nu, f32)
+    rho = np.ones(N, f32)
+    st = IncompState(u0)
+    st.p = p0
+    diag = laplacian_diag(om)
+    zero = np.zeros(N, f32)
+
+    def row(t):
+        a = analysis(om, 1.0, rho, st.u1, mu)
+        return [float(t), a[0], a[1], a[2], a[3], 0.0]
+
+    t = f32(0.0)
+    hist = [row(t)]
+    dt = adapt_dt(om, st.u1, zero, cfl_conv)
+    log_next = log_first
+    for istep in range(1, nsteps + 1):
+        bdfext3_step(om, None, st, dt, nu, maxIter=maxIter, tol=tol, pressure="reference", p_maxIter=maxIter,
+                     p_tol=tol, diag=diag)
+        t = f32(t + dt)
+        if istep == log_next:
+            hist.append(row(t))
+            log_next += log_step
+        dt = adapt_dt(om, st.u1, zero, cfl_conv)
+        if max_time is not None and t >= f32(max_time):
+            break
+    return np.array(hist), st
 
 
 def comp_tau(om: OracleMesh, csound, u):

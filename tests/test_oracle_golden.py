@@ -133,3 +133,25 @@ def test_imex_history_cpu_golden_documented_gap(case8):
     assert k == len(ref)
     assert np.max(np.abs(hist[:k, 0] - ref[:k, 0]) / np.maximum(ref[:k, 0], 1e-3)) < 0.03
     assert np.max(np.abs(hist[:k, 1] - ref[:k, 1]) / ref[:k, 1]) < 0.03
+
+
+def test_incomp_history_cpu_golden():
+    """Incompressible Taylor-Green (Tests/TGV_Incomp/CPU/AB: 8^3 order 4,
+    Re 1600, CFL 0.5, maxIter 20, tol 1e-2 for both CGs): the oracle's
+    bdfext3_main_incomp loop with conjGrad_pressure_incomp and
+    conjGrad_veloc_incomp reproduces the reference history to t = 2 (six
+    rows): EK to 1e-5 on every row, and every column within the reference's
+    own check (|cur-ref|/(|ref|+1e-4) <= 1e-4, testcheck.py:6-28) through
+    step 11; by step 41 the time (a sum of FP32 CFL steps) is 3.8e-4 off and
+    the dissipation 2.4e-4."""
+    ref = O.load_history(GOLD / "tgv_incomp_cpu_ab_8x8x8_p4.dat")
+    m = host.periodic_cube(4, 8)
+    hist, _ = O.tgv_incomp_run(O.OracleMesh(m), 1000, max_time=2.0)
+    assert hist.shape == ref.shape
+    r = rel(hist, ref)
+    print("incompressible history, max rel per column:", r.max(0))
+    assert r[:, 1].max() < 1e-5
+    assert r[:, 2:5].max() < 1e-3
+    assert r[:, 0].max() < 1e-3
+    assert r[:2].max() < 1e-5  # t = 0 and step 1 to the printed digits
+    assert r[:3].max() < 1e-4  # the reference's criterion through step 11
