@@ -193,7 +193,9 @@ int sod_gpu_conjgrad_pressure(sod_gpu_ctx *ctx, const float *Rp0, float *R, int 
 typedef struct {
   int max_iter;
   double tol;
-  int precond;         /* 0 Jacobi, 1 learned                                */
+  int precond;         /* 0 Jacobi, 1 learned; 2 (sod_gpu_incomp_step only):
+                          the reference's conjGrad_pressure_incomp in FP32
+                          with max_iter / tol, uncertified                 */
   int stagnation_window; /* iterations without a 2x residual drop -> fallback */
   int harvest;         /* 1: record (residual, error) pairs of this solve for
                           training the learned preconditioner             */
@@ -286,6 +288,16 @@ int sod_gpu_incomp_set_veloc_solver(sod_gpu_ctx *ctx, int maxIter, double tol);
 int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *ctx, int *iters, double *res_rel);
 /* Copies of the current velocity u(npoin,3) (FP32) and pressure (FP64); NULL skips. */
 int sod_gpu_incomp_get(sod_gpu_ctx *ctx, float *u, double *p);
+/* Pressure of the initial state (FP64, device), the first step's pr(:,1). */
+int sod_gpu_incomp_set_pressure(sod_gpu_ctx *ctx, const double *p);
+/* Convective CFL time step of the current velocity (host *dt):
+ * adapt_dt_cfl with zero sound speed, as CFDSolverPeriodicIncomp_evalDt
+ * (src/lib_mainBaseClass/sources/CFDSolverPeriodicIncomp.f90:119-128). */
+int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *ctx, float cfl_conv, float *dt);
+/* volAvg_EK and visc_dissipationRate of the current velocity (rho = 1,
+ * mu_fluid = nu, no entropy viscosity): out (host) = EK, eps_S, eps_D,
+ * eps_T (src/lib_sod2d/sources/mod_analysis.f90:10-144). */
+int sod_gpu_incomp_analysis(sod_gpu_ctx *ctx, double *out);
 
 /* ---- compressible time integration with library-owned state ----------
  * The conserved state lives on the device in FP64 (fp64_state = 1) or in

@@ -111,6 +111,10 @@ struct sod_gpu_ctx {
     double v_tol = 1e-4;
     int v_iters = 0;     // statistics of the last velocity solve
     double v_res = 0.0;
+    // reference-arithmetic pressure solve and the case's dt / analysis
+    float *rhs32 = nullptr, *one = nullptr, *zero = nullptr, *zeroE = nullptr, *part = nullptr;
+    double *sums = nullptr;
+    unsigned *bits = nullptr;
   } inc;
   // implicit velocity solve (conjGrad_veloc_incomp)
   struct Velo {
@@ -2176,6 +2180,15 @@ __global__ void k_poisson_rhs(int npoin_w, const int *__restrict__ lpoin_w, cons
   x[i] = nhist >= 2 ? 2.0 * p[i] - pold[i] : (nhist == 1 ? p[i] : 0.0);
 }
 
+// FP32 b = (-g0 div) / dt, the reference's pr(:,2) (time_integ_incomp.f90:351-353)
+__global__ void k_poisson_rhs32(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ div, float g0,
+                                float dt, float *__restrict__ b) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  b[i] = __fdiv_rn(__fmul_rn(-g0, div[i]), dt);
+}
+
 // u2 = (u2 - dt gradP / g0) Ml, time_integ_incomp.f90:390-394 (no wall model)
 __global__ void k_veloc_rhs(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
                             const float *__restrict__ Ml, const float *__restrict__ gp, float dt, float g0,
@@ -2373,8 +2386,15 @@ int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
       if ((rc = c->alloc(&a, 3 * N))) return rc;
     if ((rc = c->alloc(&I.div, N)) || (rc = c->alloc(&I.grad, 3 * N)) || (rc = c->alloc(&I.pf, N)) ||
         (rc = c->alloc(&I.mu, N)) || (rc = c->alloc(&I.p, N)) || (rc = c->alloc(&I.pold, N)) ||
-        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)))
+        (rc = c->alloc(&I.b, N)) || (rc = c->alloc(&I.x, N)) || (rc = c->alloc(&I.rhs32, N)) ||
+        (rc = c->alloc(&I.one, N)) || (rc = c->alloc(&I.zero, N)) ||
+        (rc = c->alloc(&I.zeroE, (size_t)c->nelem * c->N)) || (rc = c->alloc(&I.part, 3 * (size_t)c->nelem)) ||
+        (rc = c->alloc(&I.sums, 4)) || (rc = c->alloc(&I.bits, 4)))
       return rc;
+    k_fill<<<nblk((long long)N, 256), 256, 0, c->stream>>>((long long)N, 1.0f, I.one);
+    CUDA_TRY(cudaMemsetAsync(I.zero, 0, N * 4, c->stream));
+    CUDA_TRY(cudaMemsetAsync(I.zeroE, 0, (size_t)c->nelem * c->N * 4, c->stream));
+    CUDA_TRY(cudaMemsetAsync(I.rhs32, 0, N * 4, c->stream));
     I.ready = true;
   }
   // every level starts from the initial field (CFDSolverPeriodicIncomp.f90:54-66)
@@ -2424,21 +2444,51 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
   }
   rc = sod_gpu_eval_divergence(c, u2, I.div);
   if (rc) { c->async = was_async; return rc; }
-  // initial guess: the previous pressure for Jacobi (the reference's pr(:,1),
-  // mod_solver_incomp.f90:306); extrapolated from the previous two
-  // pressures for the learned path
-  const int hist = opts->precond == 1 ? I.nsteps : (I.nsteps > 0 ? 1 : 0);
-  k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, k.g0, dt, I.p, I.pold, hist, I.b, I.x);
-  c->async = was_async;
-  rc = sod_gpu_pressure_solve(c, I.b, I.x, opts, stats);
-  if (rc && rc != SOD_GPU_ESTAGNATE) return rc;
-  const int solve_rc = rc;
-  {  // pold = p; p = x
-    double *t = I.pold;
-    I.pold = I.p; I.p = I.x; I.x = t;
+  int solve_rc = 0;
+  if (opts->precond == 2) {
+    // the reference's solve: conjGrad_pressure_incomp in FP32 from the
+    // previous pressure pr(:,1), max_iter / tol, no certification
+    k_poisson_rhs32<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, k.g0, dt, I.rhs32);
+    c->async = was_async;
+    int pit = 0;
+    double pres = 0.0;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    CUDA_TRY(cudaEventRecord(e0, c->stream));
+    rc = sod_gpu_conjgrad_pressure(c, I.pf, I.rhs32, opts->max_iter, opts->tol, &pit, &pres);
+    CUDA_TRY(cudaEventRecord(e1, c->stream));
+    CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (stats) { stats->iterations = pit; stats->fallback = 0; stats->res_rel = pres; stats->seconds = ms * 1e-3; }
+    c->async = true;
+    {  // pold = p; p = (double) solution; pf = solution
+      double *t = I.pold;
+      I.pold = I.p; I.p = I.x; I.x = t;
+    }
+    k_f2d_w<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.rhs32, I.p);
+    CUDA_TRY(cudaMemcpyAsync(I.pf, I.rhs32, N * 4, cudaMemcpyDeviceToDevice, c->stream));
+  } else {
+    // initial guess: the previous pressure for Jacobi (the reference's
+    // pr(:,1), mod_solver_incomp.f90:306); extrapolated from the previous
+    // two pressures for the learned path
+    const int hist = opts->precond == 1 ? I.nsteps : (I.nsteps > 0 ? 1 : 0);
+    k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, k.g0, dt, I.p, I.pold, hist, I.b, I.x);
+    c->async = was_async;
+    rc = sod_gpu_pressure_solve(c, I.b, I.x, opts, stats);
+    if (rc && rc != SOD_GPU_ESTAGNATE) return rc;
+    solve_rc = rc;
+    {  // pold = p; p = x
+      double *t = I.pold;
+      I.pold = I.p; I.p = I.x; I.x = t;
+    }
+    c->async = true;
+    k_d2f_w<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.p, I.pf);
   }
-  c->async = true;
-  k_d2f_w<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.p, I.pf);
   rc = sod_gpu_eval_gradient(c, I.pf, I.grad);
   if (rc) { c->async = was_async; return rc; }
   k_veloc_rhs<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, I.grad, dt, k.g0, u2);
@@ -2454,6 +2504,59 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
   I.nsteps++;
   rc = c->finish();
   return rc ? rc : solve_rc;
+}
+
+int sod_gpu_incomp_set_pressure(sod_gpu_ctx *c, const double *p) {
+  if (!c || !c->inc.ready || !p) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &I = c->inc;
+  const size_t N = c->npoin;
+  CUDA_TRY(cudaMemcpyAsync(I.p, p, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(I.pold, p, N * 8, cudaMemcpyDeviceToDevice, c->stream));
+  k_d2f_w<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, I.p, I.pf);
+  return c->finish();
+}
+
+int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float *dt) {
+  if (!c || !c->inc.ready || !dt || !(cfl_conv > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &I = c->inc;
+  const unsigned init_bits = 0x56B5E621u;  // 1e14f, the reference's initial dt_conv
+  CUDA_TRY(cudaMemcpyAsync(I.bits, &init_bits, 4, cudaMemcpyHostToDevice, c->stream));
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    // zero sound speed and viscosities: only the convective limit acts
+    k_dt<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), c->helem, I.u[0], I.zero, I.zero, I.zeroE,
+                                                            I.one, cfl_conv, 1.0f, I.bits);
+    return 0;
+  });
+  unsigned b = 0;
+  CUDA_TRY(cudaMemcpyAsync(&b, I.bits, 4, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  std::memcpy(dt, &b, 4);
+  return 0;
+}
+
+int sod_gpu_incomp_analysis(sod_gpu_ctx *c, double *out) {
+  if (!c || !c->inc.ready || !out) return fail(SOD_GPU_EINVAL, "bad argument");
+  auto &I = c->inc;
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_analysis_elem<LL::P_, LL::EPB><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), I.one, I.u[0], I.mu,
+                                                                                   I.zeroE, c->Ngp_t, I.part);
+    return 0;
+  });
+  k_sum_parts<<<1, 1024, 0, c->stream>>>(c->nelem, I.part, I.sums);
+  double sums[3];
+  CUDA_TRY(cudaMemcpyAsync(sums, I.sums, 24, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const float rho0 = 1.0f, twopi = 2.0f * 3.14159f;
+  const double EK = sums[0] / (double)(rho0 * powf(twopi, 3.0f));
+  const float alpha = 1.0f / (rho0 * c->volT);
+  const double eS = sums[1] * (double)alpha, eD = (double)(4.0f / 3.0f) * sums[2] * (double)alpha;
+  out[0] = (double)(float)EK;
+  out[1] = (double)(float)eS;
+  out[2] = (double)(float)eD;
+  out[3] = (double)(float)(eS + eD);
+  return 0;
 }
 
 int sod_gpu_incomp_get(sod_gpu_ctx *c, float *u, double *p) {

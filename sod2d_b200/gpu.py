@@ -92,6 +92,9 @@ SIGNATURES = {
     "sod_gpu_incomp_step": (C.c_int, [VP, C.c_float, VP, VP]),
     "sod_gpu_incomp_get": (C.c_int, [VP, VP, VP]),
     "sod_gpu_incomp_set_veloc_solver": (C.c_int, [VP, C.c_int, C.c_double]),
+    "sod_gpu_incomp_set_pressure": (C.c_int, [VP, VP]),
+    "sod_gpu_incomp_adapt_dt": (C.c_int, [VP, C.c_float, C.POINTER(C.c_float)]),
+    "sod_gpu_incomp_analysis": (C.c_int, [VP, C.POINTER(C.c_double)]),
     "sod_gpu_incomp_veloc_stats": (C.c_int, [VP, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "sod_gpu_species_tau": (C.c_int, [VP, VP, VP]),
     "sod_gpu_eval_tau_veloc": (C.c_int, [VP] * 5),
@@ -245,6 +248,67 @@ class CompSolver:
         t = [torch.zeros(k, device="cuda") for k in (N, 3 * N, N, E * n)]
         self.ctx.call("sod_gpu_comp_get_state", *(dptr(x) for x in t))
         return dict(zip(("rho", "q", "E", "mu_e"), (x.cpu().numpy() for x in t)))
+
+    def close(self):
+        self.ctx.close()
+
+
+class IncompSolver:
+    """Incompressible periodic time loop on the GPU through the C-ABI: the
+    Taylor-Green initial state of TGVSolverIncomp (velocity and pressure),
+    the convective CFL dt of CFDSolverPeriodicIncomp_evalDt and one
+    sod_gpu_incomp_step (bdfext3_main_incomp) per step.  opts is a
+    SolveOpts for the pressure solve (precond 2: the reference's FP32 CG);
+    veloc = (maxIter, tol) of the velocity solve."""
+
+    def __init__(self, mesh, Re=1600.0, cfl_conv=0.5, veloc=(20, 1e-2)):
+        import torch
+        self.torch = torch
+        self.mesh = mesh
+        self.ctx = Context(mesh, default_phys())
+        N = mesh.npoin
+        x, y, z = (mesh.coord[i * N:(i + 1) * N].astype(np.float32) for i in range(3))
+        u0 = np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),
+                             np.zeros(N, np.float32)]).astype(np.float32)
+        p0 = (np.float32(1.0 / 16.0) * (np.cos(np.float32(2) * x) + np.cos(np.float32(2) * y)) *
+              (np.cos(np.float32(2) * z) + np.float32(2))).astype(np.float32)
+        du = torch.from_numpy(u0).cuda()
+        dp = torch.from_numpy(p0.astype(np.float64)).cuda()
+        self.nu = float(np.float32(1.0) / np.float32(Re))
+        self.ctx.call("sod_gpu_incomp_init", dptr(du), self.nu)
+        self.ctx.call("sod_gpu_incomp_set_pressure", dptr(dp))
+        self.ctx.call("sod_gpu_incomp_set_veloc_solver", int(veloc[0]), float(veloc[1]))
+        self.cfl = cfl_conv
+        self.time = np.float32(0.0)
+        self.dt = self.adapt_dt()
+        self.stats = SolveStats()
+
+    def adapt_dt(self) -> float:
+        v = C.c_float()
+        self.ctx.call("sod_gpu_incomp_adapt_dt", self.cfl, C.byref(v))
+        return float(v.value)
+
+    def analysis(self):
+        out = (C.c_double * 4)()
+        self.ctx.call("sod_gpu_incomp_analysis", out)
+        return [float(self.time)] + list(out) + [0.0]
+
+    def step(self, opts):
+        self.ctx.call("sod_gpu_incomp_step", float(self.dt), C.byref(opts), C.byref(self.stats))
+        self.time = np.float32(self.time + np.float32(self.dt))
+
+    def run(self, nsteps, opts, log_first=1, log_step=10, max_time=None):
+        hist = [self.analysis()]
+        log_next = log_first
+        for istep in range(1, nsteps + 1):
+            self.step(opts)
+            if istep == log_next:
+                hist.append(self.analysis())
+                log_next += log_step
+            self.dt = self.adapt_dt()
+            if max_time is not None and self.time >= np.float32(max_time):
+                break
+        return np.array(hist)
 
     def close(self):
         self.ctx.close()

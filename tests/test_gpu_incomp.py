@@ -164,3 +164,29 @@ def test_incomp_step_arguments(gpu):
     with pytest.raises(RuntimeError):
         ctx.call("sod_gpu_incomp_veloc_stats", None, None)  # state not initialised
     ctx.close()
+
+
+def test_tgv_incomp_reference_history(gpu):
+    """The incompressible Taylor-Green loop on the GPU in the reference's
+    own arithmetic (Tests/TGV_Incomp/CPU/AB: 8^3 order 4, Re 1600, CFL 0.5,
+    FP32 pressure CG and velocity CG with maxIter 20, tol 1e-2; dt, step and
+    analysis through the C-ABI) against the oracle's loop and the reference
+    history: EK to 1e-5 on every row, every column within the reference's
+    criterion (1e-4) through step 11 and within 5e-4 to t = 2 (the time
+    column sums FP32 CFL steps whose max |u| rounds differently)."""
+    from pathlib import Path
+    gold = O.load_history(Path(__file__).resolve().parent / "golden" / "tgv_incomp_cpu_ab_8x8x8_p4.dat")
+    m = host.periodic_cube(4, 8)
+    ohist, _ = O.tgv_incomp_run(O.OracleMesh(m), 1000, max_time=2.0)
+    s = gpu.IncompSolver(m, Re=1600.0, cfl_conv=0.5, veloc=(20, 1e-2))
+    hist = s.run(1000, gpu.SolveOpts(20, 1e-2, 2, 50, 0), max_time=2.0)
+    s.close()
+    rel = lambda a, b: np.abs(a - b) / (np.abs(b) + 1e-4)
+    assert hist.shape == gold.shape == ohist.shape
+    print("GPU vs oracle, max rel per column:", rel(hist, ohist).max(0))
+    print("GPU vs reference history, max rel per column:", rel(hist, gold).max(0))
+    for ref in (ohist, gold):
+        r = rel(hist, ref)
+        assert r[:, 1].max() < 1e-5
+        assert r[:3].max() < 1e-4
+        assert r.max() < 5e-4
