@@ -72,15 +72,16 @@ def test_fp64_state_close_to_fp32(gpu):
     assert rel(hb, ha).max() < 1e-4
 
 
-@pytest.mark.parametrize("stages", [4, 3])
-def test_imex_history_matches_oracle(gpu, stages):
+@pytest.mark.parametrize("porder,Ma,stages", [(4, 1.25, 4), (4, 1.25, 3), (3, 0.1, 4)])
+def test_imex_history_matches_oracle(gpu, porder, Ma, stages):
     """IMEX integrator (imex_main with conjGrad_imex) on the reference's
-    IMEX test case (8^3 order-4 cube, Ma = 1.25, CFL 0.95): the GPU
+    IMEX test case (8^3 order-4 cube, Ma = 1.25, CFL 0.95) and on an
+    order-3 cube at Ma = 0.1: the GPU
     analysis rows agree with the oracle's to 1e-4 relative, the final
     conserved fields to 1e-5 relative L2; with stages = 4 the first step's
     time is the reference history's."""
-    m = host.periodic_cube(4, 8)
-    ic = host.tgv_comp_init(m, Ma=1.25)
+    m = host.periodic_cube(porder, 8)
+    ic = host.tgv_comp_init(m, Ma=Ma)
     om = O.OracleMesh(m)
     nsteps = 21
     prm = O.comp_params(ic, cfl_conv=0.95, cfl_diff=1000.5, stages=stages, imex=True, first_mue=True)
@@ -100,7 +101,7 @@ def test_imex_history_matches_oracle(gpu, stages):
     for k in ("rho", "E"):
         assert rel_l2(fin[k][w], ref_fin[k][w]) < 1e-5, k
     assert its.value >= stages - 1 and res.value < 1e-3
-    if stages == 4:
+    if stages == 4 and porder == 4:
         gold = O.load_history(GOLD / "tgv_comp_cpu_imex4_8x8x8_p4.dat")
         assert abs(hist[1, 0] - gold[1, 0]) / gold[1, 0] < 1e-6
 
