@@ -265,8 +265,9 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     ft_s, ft_loss, ft_pairs = 0.0, C.c_float(), 0
     for i, (name, kind) in enumerate((("jacobi", 0), ("learned", 1))):
         c = ctxs[0] if kind == 1 else ctxs[1]
-        it, ms, rmax, fb, dv, vits = [], [], 0.0, 0, [], []
+        it, ms, rmax, fb, dv, vits, step_ms = [], [], 0.0, 0, [], [], []
         vit = C.c_int()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         if kind == 1 and self_steps > 0:
             c.call("sod_gpu_precond_restart_harvest")
         for k in range(compare_steps):
@@ -276,7 +277,11 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
                 c.call("sod_gpu_precond_train", ft_steps, ft_batch, ft_lr, 11, C.byref(ft_loss))
                 ft_s = time.perf_counter() - t0
             o = gpu.SolveOpts(50000, 1e-8, kind, 200, 1 if (kind == 1 and k < self_steps) else 0)
+            ev[0].record()
             c.call("sod_gpu_incomp_step", dt, C.byref(o), C.byref(st))
+            ev[1].record()
+            ev[1].synchronize()
+            step_ms.append(ev[0].elapsed_time(ev[1]))
             it.append(st.iterations)
             ms.append(st.seconds * 1e3)
             rmax = max(rmax, st.res_rel)
@@ -289,6 +294,7 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
             vits.append(vit.value)
         res[name] = {"mean_iterations": round(float(np.mean(it)), 1), "mean_solve_ms": round(float(np.mean(ms)), 3),
                      "mean_velocity_cg_iterations": round(float(np.mean(vits)), 2),
+                     "mean_step_ms": round(float(np.mean(step_ms)), 3),
                      "max_true_residual": rmax, "fallbacks": fb, "mean_div_u_l2": float(np.mean(dv)),
                      "mean_solve_ms_first_100": round(float(np.mean(ms[:100])), 3),
                      "iterations_every_50_steps": it[::50]}
