@@ -214,7 +214,7 @@ def run_reference(args, rank, world):
             "unit": "Mnode-stages/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(1e3 * sum(times) / len(times), 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": workload_config(),
+            "data": "synthetic", "config": workload_config(args.nelem1d),
             "cpu_baseline": info, "e2e": {"value": round(v, 3), "unit": "Mnode-stages/s", "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -418,12 +418,18 @@ def precision_study(nelem1d=16, nsteps=200, porder=3, Ma=0.1, stages=4):
     return out
 
 
-def workload_config():
-    return {"workload": f"RHS micro-benchmark: periodic cube {NELEM_1D}^3 HEX64 (p=3), interior GLL nodes jittered "
+def workload_config(nelem1d=NELEM_1D):
+    ne = nelem1d ** 3
+    nw = (PORDER * nelem1d) ** 3
+    state_mb = nw * 5 * 4 / 1e6                   # rho, q(3), E in FP32
+    geo_mb = ne * (PORDER + 1) ** 3 * 10 * 4 / 1e6  # J^-1 (9) + gpvol per Gauss point
+    slots_gb = 1.6 * ne / 64 ** 3                   # element slots of both passes, 1.6 GB at 64^3
+    l2 = "inputs larger than L2" if state_mb + geo_mb > 126 else "inputs partly L2-resident"
+    return {"workload": f"RHS micro-benchmark: periodic cube {nelem1d}^3 HEX64 (p=3), interior GLL nodes jittered "
                         f"+-5%, random FP32 state, fused convective+diffusive(LPS)+entropy-viscosity residual with "
                         f"assembly and lumped-mass inversion",
-            "nelem": NELEM_1D ** 3, "porder": PORDER, "working_nodes": (PORDER * NELEM_1D) ** 3,
-            "l2": "inputs larger than L2 (state 142 MB, geometry 671 MB, assembly slots 1.6 GB)",
+            "nelem": ne, "porder": PORDER, "working_nodes": nw,
+            "l2": f"{l2} (state {state_mb:.0f} MB, geometry {geo_mb:.0f} MB, assembly slots {slots_gb:.2f} GB)",
             "parallelism": "replicas"}
 
 
@@ -589,7 +595,7 @@ def main():
         "metric": "Mnode-stages/s (fused compressible RHS, FP32)", "value": round(value, 2),
         "unit": "Mnode-stages/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": workload_config(),
+        "dtype": "f32", "data": "synthetic", "config": workload_config(args.nelem1d),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": int(round(DRAM_B_PER_NODE_STAGE * m.npoin_w)),
