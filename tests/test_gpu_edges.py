@@ -140,3 +140,32 @@ def test_zero_rhs_gives_zero_solution(gpu):
     assert st.iterations == 0
     assert float(x.abs().max()) == 0.0
     ctx.close()
+
+
+def test_new_step_entries_reject_missing_state(gpu):
+    """The incompressible and IMEX entries refuse to run before their state
+    exists, and refuse bad arguments, with an error status (no kernel runs
+    on an unset state)."""
+    m = host.periodic_cube(3, 2, seed=5)
+    ctx = gpu.Context(m, gpu.default_phys())
+    dt, out4 = C.c_float(), (C.c_double * 4)()
+    its, res = C.c_int(), C.c_double()
+    for name, args in (("sod_gpu_incomp_adapt_dt", (0.5, C.byref(dt))), ("sod_gpu_incomp_analysis", (out4,)),
+                       ("sod_gpu_incomp_set_pressure", (None,)), ("sod_gpu_incomp_get", (None, None)),
+                       ("sod_gpu_comp_imex_step", (1e-3, 200, 1e-3)),
+                       ("sod_gpu_comp_imex_stats", (C.byref(its), C.byref(res)))):
+        with pytest.raises(RuntimeError):
+            ctx.call(name, *args)
+    N = m.npoin
+    u = torch.zeros(3 * N, device="cuda")
+    ctx.call("sod_gpu_incomp_init", gpu.dptr(u), 0.01)
+    with pytest.raises(RuntimeError):  # non-positive CFL
+        ctx.call("sod_gpu_incomp_adapt_dt", 0.0, C.byref(dt))
+    with pytest.raises(RuntimeError):  # unknown preconditioner kind
+        ctx.call("sod_gpu_incomp_step", 0.01, C.byref(gpu.SolveOpts(20, 1e-8, 3, 50, 0)), C.byref(gpu.SolveStats()))
+    # a zero velocity field: analysis is zero, dt is the initial 1e14
+    ctx.call("sod_gpu_incomp_analysis", out4)
+    assert list(out4) == [0.0, 0.0, 0.0, 0.0]
+    ctx.call("sod_gpu_incomp_adapt_dt", 0.5, C.byref(dt))
+    assert dt.value > 1e13
+    ctx.close()
