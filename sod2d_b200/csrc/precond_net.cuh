@@ -220,17 +220,28 @@ k_patch_apply(long long nelem, const int *__restrict__ pt, const double *__restr
 //   H[16 x K] = X[16 x NP] B^T,  Y = gains * H,  O[16 x NP] = Y B.
 // Operands are staged in shared memory with row strides chosen so that the
 // fragment loads are free of bank conflicts.
+// The B fragment of an m16n8k8 step is the pair (k0 + t, k0 + t + 4) of the
+// k index; both copies of B in shared memory store each block of 8 k values
+// in the order 0 4 1 5 2 6 3 7, so that the pair is one aligned 8-byte load.
+// Row strides of 8 or 24 mod 32 words keep those loads free of bank
+// conflicts.
+__host__ __device__ constexpr int kpair_pos(int k) {
+  const int r = k & 7;
+  return (k & ~7) | (r < 4 ? 2 * r : 2 * (r - 4) + 1);
+}
+__host__ __device__ constexpr int stride_8_24(int n) { return n + ((8 - n % 16) + 16) % 16; }
+
 template <int P>
 struct TcDims {
   using D = NetDims<P>;
   static constexpr int KP = (D::NP + 7) / 8 * 8;                   // slots padded to the mma k/n step
-  static constexpr int S1 = KP + 4;                                // B as [mode][slot]: stride = 4 mod 8
-  static constexpr int S2 = KP + ((8 - KP % 16) + 16) % 16;        // B as [mode][slot]: stride = 8 or 24 mod 32
+  static constexpr int S1 = stride_8_24(KP);                       // B as [mode][slot, paired]
+  static constexpr int S2 = stride_8_24(NET_K);                    // B as [slot][mode, paired]
   static constexpr int SY = NET_K + 4;                             // Y tile [16][SY]
   static constexpr int WARPS = 16;                                 // one block per SM
   static constexpr int KC = 10;                                    // k-steps whose operands are gathered together
   static constexpr int NC = 10;                                    // output n-tiles whose positions are loaded together
-  static constexpr size_t smem() { return (size_t)(NET_K * S1 + NET_K * S2 + WARPS * 16 * SY) * 4; }
+  static constexpr size_t smem() { return (size_t)(NET_K * S1 + KP * S2 + WARPS * 16 * SY) * 4; }
 };
 
 __device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
@@ -268,12 +279,12 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restr
   extern __shared__ __align__(16) float smem[];
   float *B1 = smem, *B2 = B1 + K * T::S1;
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  float *Y = B2 + K * T::S2 + warp * 16 * T::SY;
+  float *Y = B2 + KP * T::S2 + warp * 16 * T::SY;
   for (int i = threadIdx.x; i < K * KP; i += blockDim.x) {
     const int k = i / KP, j = i % KP;
     const float b = j < NP ? prm[D::O_B + k * NP + j] : 0.f;
-    B1[k * T::S1 + j] = b;
-    B2[k * T::S2 + j] = b;
+    B1[k * T::S1 + kpair_pos(j)] = b;
+    B2[j * T::S2 + kpair_pos(k)] = b;
   }
   __syncthreads();
   const int g = lane >> 2, t = lane & 3;
@@ -314,10 +325,9 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restr
         const int k0 = (c0 + kk) * 8;
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-          const uint32_t b0 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t]);
-          const uint32_t b1 = __float_as_uint(B1[(nt * 8 + g) * T::S1 + k0 + t + 4]);
+          const float2 bb = *reinterpret_cast<const float2 *>(B1 + (nt * 8 + g) * T::S1 + k0 + 2 * t);
           mma_tf32(h[nt], __float_as_uint(xv[kk][0]), __float_as_uint(xv[kk][1]), __float_as_uint(xv[kk][2]),
-                   __float_as_uint(xv[kk][3]), b0, b1);
+                   __float_as_uint(xv[kk][3]), __float_as_uint(bb.x), __float_as_uint(bb.y));
         }
       }
     }
@@ -366,9 +376,8 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restr
 #pragma unroll
         for (int kk = 0; kk < 4; ++kk) {
           const int k0 = kk * 8;
-          const uint32_t b0 = __float_as_uint(B2[(k0 + t) * T::S2 + nt * 8 + g]);
-          const uint32_t b1 = __float_as_uint(B2[(k0 + t + 4) * T::S2 + nt * 8 + g]);
-          mma_tf32(o, a[kk][0], a[kk][1], a[kk][2], a[kk][3], b0, b1);
+          const float2 bb = *reinterpret_cast<const float2 *>(B2 + (nt * 8 + g) * T::S2 + k0 + 2 * t);
+          mma_tf32(o, a[kk][0], a[kk][1], a[kk][2], a[kk][3], __float_as_uint(bb.x), __float_as_uint(bb.y));
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q)
