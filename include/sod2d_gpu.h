@@ -299,6 +299,26 @@ int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *ctx, float cfl_conv, float *dt);
  * eps_T (src/lib_sod2d/sources/mod_analysis.f90:10-144). */
 int sod_gpu_incomp_analysis(sod_gpu_ctx *ctx, double *out);
 
+/* ---- entropy viscosity, individually (device pointers, reference layout) */
+/* generic_scalar_convec_ijk, src/lib_sod2d/sources/elem_convec.f90:472-594:
+ * assembled split-form residual of a scalar eta with flux q(npoin,3) and
+ * velocity u(npoin,3) into R(npoin) (zeroed first when initialze != 0),
+ * scaled by fact; not mass-inverted. */
+int sod_gpu_generic_scalar_convec_ijk(sod_gpu_ctx *ctx, const float *q, const float *eta, const float *u, float *R,
+                                      int initialze, float fact);
+/* smart_visc_spectral_imex, src/lib_sod2d/sources/mod_entropy_viscosity.f90:
+ * 113-227 (high-Mach path): mu_e(nelem,ngaus) from the entropy residual
+ * Reta(npoin), rho, u, csound; needs helem at init. */
+int sod_gpu_smart_visc_spectral_imex(sod_gpu_ctx *ctx, const float *Reta, const float *rho, const float *u,
+                                     const float *csound, float *mu_e);
+/* ducros_visc_limit, src/lib_sod2d/sources/mod_entropy_viscosity.f90:277-314:
+ * mu_e(nelem,ngaus) (in/out) scaled by the Ducros sensor of divU (assembled,
+ * eval_divergence), vorti(npoin,3) (compute_vorticity) and |u| / helem_l;
+ * rho and csound only feed a quantity the reference discards.  Needs helem_l
+ * at init. */
+int sod_gpu_ducros_visc_limit(sod_gpu_ctx *ctx, const float *rho, const float *u, const float *divU,
+                              const float *vorti, const float *csound, float *mu_e);
+
 /* ---- compressible time integration with library-owned state ----------
  * The conserved state lives on the device in FP64 (fp64_state = 1) or in
  * FP32 (fp64_state = 0, the reference's USE_RP=4 arithmetic); the element

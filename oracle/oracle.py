@@ -79,6 +79,12 @@ def lib() -> C.CDLL:
             getattr(_lib, f"oracle_cg_veloc_{s}").argtypes = ([C.POINTER(MeshT), real, real] + [C.c_void_p] * 4 +
                                                               [C.c_int, C.c_double, C.c_void_p])
             getattr(_lib, f"oracle_cg_veloc_{s}").restype = C.c_int
+            getattr(_lib, f"oracle_scalar_convec_{s}").argtypes = ([C.POINTER(MeshT)] + [C.c_void_p] * 4 +
+                                                                   [C.c_int, C.c_double])
+            for nm, na in (("smart_visc", 5), ("ducros", 6), ("vorticity", 2)):
+                getattr(_lib, f"oracle_{nm}_{s}").argtypes = [C.POINTER(MeshT)] + [C.c_void_p] * na
+            for nm in ("scalar_convec", "smart_visc", "ducros", "vorticity"):
+                getattr(_lib, f"oracle_{nm}_{s}").restype = C.c_int
     return _lib
 
 
@@ -408,6 +414,38 @@ def tgv_incomp_run(om, nsteps, Re=1600.0, cfl_conv=0.5, maxIter=20, tol=1e-2, lo
         if max_time is not None and t >= f32(max_time):
             break
     return np.array(hist), st
+
+
+def scalar_convec(om, q, eta, u, R=None, init=True, fact=1.0):
+    """generic_scalar_convec_ijk, elem_convec.f90:472-594 (not mass-inverted)."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = np.zeros(om.mesh.npoin, om.dtype) if R is None else c(R).copy()
+    keep = [c(q), c(eta), c(u)]
+    om.fn("scalar_convec")(C.byref(om.s), *(_p(a) for a in keep), _p(out), int(init), float(fact))
+    return out
+
+
+def smart_visc(om, Reta, rho, u, csound):
+    """smart_visc_spectral_imex, mod_entropy_viscosity.f90:113-227: mu_e (nelem*ngaus)."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = np.zeros(om.mesh.nelem * om.mesh.nnode, om.dtype)
+    keep = [c(Reta), c(rho), c(u), c(csound)]
+    om.fn("smart_visc")(C.byref(om.s), *(_p(a) for a in keep), _p(out))
+    return out
+
+
+def ducros(om, rho, u, divU, vorti, csound, mu_e):
+    """ducros_visc_limit, mod_entropy_viscosity.f90:277-314: limited copy of mu_e."""
+    c = lambda a: np.ascontiguousarray(a, om.dtype)
+    out = c(mu_e).copy()
+    keep = [c(rho), c(u), c(divU), c(vorti), c(csound)]
+    om.fn("ducros")(C.byref(om.s), *(_p(a) for a in keep), _p(out))
+    return out
+
+
+def vorticity(om, u):
+    """compute_vorticity with the per-node averaging, mod_operators.f90:684-775."""
+    return _op(om, "vorticity", 3, u)
 
 
 def comp_tau(om: OracleMesh, csound, u):

@@ -696,3 +696,37 @@ ORACLE_BOTH(DEF_INCOMP)
 ORACLE_BOTH(DEF_VELOC)
 
 }  // extern "C"
+
+// Entropy-viscosity pieces, individually (generic_scalar_convec_ijk,
+// smart_visc_spectral_imex, ducros_visc_limit, compute_vorticity).
+#define DEF_ENTROPY(R, S)                                                                              \
+  int oracle_scalar_convec_##S(const oracle_mesh_t *cm, const R *q, const R *eta, const R *u, R *Rout, \
+                               int init, double fact) {                                                \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    generic_scalar_convec_ijk<R>(m, g, q, eta, u, Rout, init != 0, (R)fact);                           \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_smart_visc_##S(const oracle_mesh_t *cm, const R *Reta, const R *rho, const R *u,          \
+                            const R *csound, R *mu_e) {                                                \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    smart_visc_spectral_imex<R>(m, g, Reta, rho, u, csound, mu_e);                                     \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_ducros_##S(const oracle_mesh_t *cm, const R *rho, const R *u, const R *divU,              \
+                        const R *vorti, const R *csound, R *mu_e) {                                    \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    ducros_visc_limit<R>(m, g, rho, u, divU, vorti, csound, mu_e);                                     \
+    return 0;                                                                                          \
+  }                                                                                                    \
+  int oracle_vorticity_##S(const oracle_mesh_t *cm, const R *u, R *vorti) {                            \
+    Mesh m = make_mesh(cm);                                                                            \
+    Geo<R> g = make_geo<R>(cm);                                                                        \
+    compute_vorticity<R>(m, g, u, vorti);                                                              \
+    return 0;                                                                                          \
+  }
+extern "C" {
+ORACLE_BOTH(DEF_ENTROPY)
+}

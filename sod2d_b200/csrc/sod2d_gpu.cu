@@ -59,6 +59,7 @@ struct sod_gpu_ctx {
   float *geo = nullptr, *Dnat = nullptr, *invMl = nullptr, *Ml = nullptr, *helem = nullptr, *helem_l_t = nullptr;
   // scratch
   float *slotsA = nullptr, *slotsB = nullptr, *proj12 = nullptr, *mue_t = nullptr, *musgs_t = nullptr;
+  unsigned *vbits = nullptr;  // minimum density of the standalone smart_visc_spectral_imex
   size_t bytes = 0;
   std::vector<void *> allocs;
   std::vector<void *> host_allocs;  // pinned host memory
@@ -1314,6 +1315,58 @@ void comp_visc(sod_gpu_ctx *c, const float *Reta, const float *rho, const float 
 }  // namespace
 
 extern "C" {
+
+int sod_gpu_generic_scalar_convec_ijk(sod_gpu_ctx *c, const float *q, const float *eta, const float *u, float *R,
+                                      int initialze, float fact) {
+  if (!c || !q || !eta || !u || !R) return fail(SOD_GPU_EINVAL, "bad argument");
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_entropy_elem<LL::P_, LL::EPB, false><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), q, eta, u,
+                                                                                        nullptr, c->slotsB, fact);
+    return 0;
+  });
+  OutPtrs o{};
+  o.p[0] = R;
+  k_gather<8, 1, false><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, nullptr, o,
+                                                                     initialze ? 0 : 1, 0);
+  return c->finish();
+}
+
+int sod_gpu_smart_visc_spectral_imex(sod_gpu_ctx *c, const float *Reta, const float *rho, const float *u,
+                                     const float *csound, float *mu_e) {
+  if (!c || !Reta || !rho || !u || !csound || !mu_e) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (!c->helem) return fail(SOD_GPU_EINVAL, "smart_visc_spectral_imex needs helem at init");
+  int rc;
+  if (!c->vbits && (rc = c->alloc(&c->vbits, 4))) return rc;
+  const unsigned init_bits = 0x47C35000u;  // 100000.0f, the reference's initial minimum
+  CUDA_TRY(cudaMemcpyAsync(c->vbits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+  k_min_rho<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, c->vbits);
+  ViscArgs V{};
+  V.Reta = Reta; V.rho = rho; V.u = u; V.csound = csound; V.Ml = c->Ml;
+  V.helem = c->helem; V.helem_l_t = c->helem_l_t; V.min_rho_bits = c->vbits;
+  V.ce = c->phys.ce; V.cmax = c->phys.cmax; V.cglob = c->phys.cglob; V.ducros_min = c->phys.ducros_min_val;
+  V.inv_p = 1.0f / (float)c->P; V.ducros = 0;
+  // the element-layout copy goes to scratch: the context's own mu_e is left alone
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_visc<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), V, c->a_of_t, c->slotsA, mu_e);
+    return 0;
+  });
+  return c->finish();
+}
+
+int sod_gpu_ducros_visc_limit(sod_gpu_ctx *c, const float *rho, const float *u, const float *divU,
+                              const float *vorti, const float *csound, float *mu_e) {
+  if (!c || !rho || !u || !divU || !vorti || !csound || !mu_e) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (!c->helem_l_t) return fail(SOD_GPU_EINVAL, "ducros_visc_limit needs helem_l at init");
+  dispatch(c, [&](auto L) {
+    using LL = decltype(L);
+    k_ducros<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), u, divU, vorti, c->Ml, c->helem_l_t,
+                                                               c->phys.ducros_min_val, c->a_of_t, mu_e);
+    return 0;
+  });
+  return c->finish();
+}
 
 int sod_gpu_comp_init_state(sod_gpu_ctx *c, const sod_rk_cfg_t *cfg, const float *rho, const float *u,
                             const float *q, const float *pr, const float *E, const float *Tem, const float *csound,

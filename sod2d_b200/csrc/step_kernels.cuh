@@ -104,7 +104,8 @@ __global__ void k_feta(int npoin_w, long long npoin, const int *__restrict__ lpo
 template <int P, int EPB, bool WANT_DC>
 __global__ void __launch_bounds__(EPB *Cfg<P>::NT)
 k_entropy_elem(MeshDev m, const float *__restrict__ feta, const float *__restrict__ eta1,
-               const float *__restrict__ u1, const float *__restrict__ u2, float *__restrict__ slots) {
+               const float *__restrict__ u1, const float *__restrict__ u2, float *__restrict__ slots,
+               float fact = 1.0f) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT, NF = 10;
   __shared__ __align__(16) float sm[EPB][NF][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
@@ -149,7 +150,7 @@ k_entropy_elem(MeshDev m, const float *__restrict__ feta, const float *__restric
   float Re = 0.5f * (divFe + etal * divU);
 #pragma unroll
   for (int a = 0; a < 3; ++a) Re = Re + 0.5f * (sm[el][1 + a][t] * gradE[a]);
-  float out[5] = {gv * Re, 0.f, 0.f, 0.f, 0.f};
+  float out[5] = {fact * (gv * Re), 0.f, 0.f, 0.f, 0.f};
   if (WANT_DC) {
     float gu[3][3];
 #pragma unroll
@@ -273,6 +274,37 @@ __global__ void k_visc(MeshDev m, ViscArgs A, const int *__restrict__ a_of_t, fl
     }
     mue_t[e * N + t] = mu;
     if (mue_ref) mue_ref[e + m.nelem * a_of_t[t]] = mu;
+  }
+}
+
+// ducros_visc_limit, mod_entropy_viscosity.f90:277-314, on a given mu_e in
+// the reference's (nelem, ngaus) layout: mu_e *= max(phi - min, 0) phi2 +
+// min with phi, phi2 from div u / Ml, the vorticity and |u| / helem_l (the
+// reference's betae is computed there but unused).  Warp per element.
+template <int P>
+__global__ void k_ducros(MeshDev m, const float *__restrict__ u, const float *__restrict__ divU,
+                         const float *__restrict__ vort, const float *__restrict__ Ml,
+                         const float *__restrict__ helem_l_t, float ducros_min, const int *__restrict__ a_of_t,
+                         float *__restrict__ mue_ref) {
+  constexpr int N = Cfg<P>::N;
+  const long long e = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x % 32;
+  if (e >= m.nelem) return;
+  const long long NP = m.npoin;
+  for (int t = lane; t < N; t += 32) {
+    const int p = m.conn[e * N + t];
+    const float divUl = divU[p] / Ml[p];
+    const float u0 = u[p], u1 = u[p + NP], u2 = u[p + 2 * NP];
+    const float aux2 = sqrtf(u0 * u0 + u1 * u1 + u2 * u2);
+    const float v0 = vort[p], v1 = vort[p + NP], v2 = vort[p + 2 * NP];
+    const float vv = v0 * v0 + v1 * v1 + v2 * v2;
+    const float d2 = divUl * divUl;
+    const float eps = 1.1920929e-07f;  // epsilon(1.0) of real(4)
+    const float phi = fminf((4.0f / 3.0f) * d2 / (d2 + vv + eps), 1.0f);
+    const float hl = 1.0f * aux2 / helem_l_t[e * N + t];
+    const float phi2 = d2 / (d2 + hl * hl + eps);
+    float &mu = mue_ref[e + m.nelem * a_of_t[t]];
+    mu = mu * (fmaxf(phi - ducros_min, 0.f) * phi2 + ducros_min);
   }
 }
 
