@@ -319,6 +319,15 @@ int sod_gpu_smart_visc_spectral_imex(sod_gpu_ctx *ctx, const float *Reta, const 
 int sod_gpu_ducros_visc_limit(sod_gpu_ctx *ctx, const float *rho, const float *u, const float *divU,
                               const float *vorti, const float *csound, float *mu_e);
 
+/* The stage update of rk_4_ls_main on the caller's FP32 arrays (working
+ * nodes): first != 0: U2 += (gam dt) R (time_integ_ls.f90:325-329, U1 may be
+ * NULL); otherwise U2 = lam1 U1 + lami U2 + (gam dt) R (:352-356), with
+ * lam1 = lambda_ij(istep+1,1), lami = lambda_ij(istep+1,istep), gam =
+ * gamma_ij(istep+1,istep).  Fields rho, q(npoin,3), E; R* mass-inverted. */
+int sod_gpu_rk_ls_stage(sod_gpu_ctx *ctx, int first, float lam1, float lami, float gam, float dt, const float *rho1,
+                        const float *q1, const float *E1, float *rho2, float *q2, float *E2, const float *Rmass,
+                        const float *Rmom, const float *Rener);
+
 /* ---- compressible time integration with library-owned state ----------
  * The conserved state lives on the device in FP64 (fp64_state = 1) or in
  * FP32 (fp64_state = 0, the reference's USE_RP=4 arithmetic); the element

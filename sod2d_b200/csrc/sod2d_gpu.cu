@@ -1368,6 +1368,17 @@ int sod_gpu_ducros_visc_limit(sod_gpu_ctx *c, const float *rho, const float *u, 
   return c->finish();
 }
 
+int sod_gpu_rk_ls_stage(sod_gpu_ctx *c, int first, float lam1, float lami, float gam, float dt, const float *rho1,
+                        const float *q1, const float *E1, float *rho2, float *q2, float *E2, const float *Rmass,
+                        const float *Rmom, const float *Rener) {
+  if (!c || !rho2 || !q2 || !E2 || !Rmass || !Rmom || !Rener || (!first && (!rho1 || !q1 || !E1)))
+    return fail(SOD_GPU_EINVAL, "bad argument");
+  k_ls_stage_ref<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->npoin, c->lpoin_w, first ? 1 : 0, lam1,
+                                                               lami, gam, dt, rho1, q1, E1, rho2, q2, E2, Rmass,
+                                                               Rmom, Rener);
+  return c->finish();
+}
+
 int sod_gpu_comp_init_state(sod_gpu_ctx *c, const sod_rk_cfg_t *cfg, const float *rho, const float *u,
                             const float *q, const float *pr, const float *E, const float *Tem, const float *csound,
                             const float *machno, const float *eta) {

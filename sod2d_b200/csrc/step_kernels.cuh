@@ -308,6 +308,32 @@ __global__ void k_ducros(MeshDev m, const float *__restrict__ u, const float *__
   }
 }
 
+// Stage update of rk_4_ls_main on reference-layout FP32 arrays, working
+// nodes, five fields (rho, E, q x/y/z): first stage U2 += (gam dt) R
+// (time_integ_ls.f90:325-329), later stages U2 = l1 U1 + li U2 + (gam dt) R
+// (:352-356), rounded as the reference (no contraction).
+__global__ void k_ls_stage_ref(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, int first, float l1,
+                               float li, float gam, float dt, const float *__restrict__ rho1,
+                               const float *__restrict__ q1, const float *__restrict__ E1, float *__restrict__ rho2,
+                               float *__restrict__ q2, float *__restrict__ E2, const float *__restrict__ Rmass,
+                               const float *__restrict__ Rmom, const float *__restrict__ Rener) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const long long p = lpoin_w[t];
+  const float gdt = __fmul_rn(gam, dt);
+  auto upd = [&](float u1, float u2, float r) {
+    return first ? __fadd_rn(u2, __fmul_rn(gdt, r))
+                 : __fadd_rn(__fadd_rn(__fmul_rn(l1, u1), __fmul_rn(li, u2)), __fmul_rn(gdt, r));
+  };
+  rho2[p] = upd(first ? 0.f : rho1[p], rho2[p], Rmass[p]);
+  E2[p] = upd(first ? 0.f : E1[p], E2[p], Rener[p]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const long long k = p + npoin * d;
+    q2[k] = upd(first ? 0.f : q1[k], q2[k], Rmom[k]);
+  }
+}
+
 // Sutherland viscosity at working nodes.
 __global__ void k_sutherland(int npoin_w, const int *__restrict__ lpoin_w, float mu_factor,
                              const float *__restrict__ Tem, float *__restrict__ mu) {

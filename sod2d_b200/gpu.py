@@ -65,6 +65,7 @@ SIGNATURES = {
     "sod_gpu_generic_scalar_convec_ijk": (C.c_int, [VP] * 5 + [C.c_int, C.c_float]),
     "sod_gpu_smart_visc_spectral_imex": (C.c_int, [VP] * 6),
     "sod_gpu_ducros_visc_limit": (C.c_int, [VP] * 7),
+    "sod_gpu_rk_ls_stage": (C.c_int, [VP, C.c_int] + [C.c_float] * 4 + [VP] * 9),
     "sod_gpu_set_mu_e": (C.c_int, [VP, VP]),
     "sod_gpu_comp_init_state": (C.c_int, [VP, C.POINTER(RkCfg)] + [VP] * 9),
     "sod_gpu_comp_rk_ls_step": (C.c_int, [VP, C.c_float]),

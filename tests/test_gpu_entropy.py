@@ -84,3 +84,36 @@ def test_entropy_pieces_match_oracle(gpu, porder):
     assert err < 1e-5
     assert not np.allclose(lim_ref, mu_ref)  # the limiter acted
     ctx.close()
+
+
+def test_rk_ls_stage_bitwise(gpu):
+    """The stage update of rk_4_ls_main as its own call: bit-identical to the
+    FP32 arithmetic of time_integ_ls.f90:325-329 (first stage) and :352-356
+    (later stages) on the working nodes; other nodes untouched."""
+    m = host.periodic_cube(3, 3, seed=41)
+    N = m.npoin
+    w = m.lpoin_w - 1
+    rng = np.random.default_rng(42)
+    f32 = np.float32
+    U1 = [rng.normal(size=k * N).astype(f32) for k in (1, 3, 1)]
+    U2 = [rng.normal(size=k * N).astype(f32) for k in (1, 3, 1)]
+    R = [rng.normal(size=k * N).astype(f32) for k in (1, 3, 1)]
+    lam1, lami, gam, dt = f32(0.571403511494104), f32(0.428596488505896), f32(0.110577759392786), f32(3.7e-3)
+    ctx = gpu.Context(m, gpu.default_phys())
+    dv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    gdt = gam * dt
+    W3 = np.concatenate([w + N * d for d in range(3)])
+    for first in (1, 0):
+        d1, d2, dr = [dv(a) for a in U1], [dv(a) for a in U2], [dv(a) for a in R]
+        ctx.call("sod_gpu_rk_ls_stage", first, float(lam1), float(lami), float(gam), float(dt),
+                 *(gpu.dptr(x) for x in d1), *(gpu.dptr(x) for x in d2), *(gpu.dptr(x) for x in dr))
+        for k, idx in ((0, w), (1, W3), (2, w)):
+            got = d2[k].cpu().numpy()
+            if first:
+                exp = U2[k][idx] + gdt * R[k][idx]
+            else:
+                exp = (lam1 * U1[k][idx] + lami * U2[k][idx]) + gdt * R[k][idx]
+            assert np.array_equal(got[idx].view(np.uint32), exp.astype(f32).view(np.uint32))
+            other = np.setdiff1d(np.arange(got.size), idx)
+            assert np.array_equal(got[other], U2[k][other])
+    ctx.close()
