@@ -89,6 +89,42 @@ const char *sod_gpu_last_error(void);
 /* Device bytes held by the context (mirrors + scratch). */
 size_t sod_gpu_device_bytes(const sod_gpu_ctx *ctx);
 
+/* ---- partitioned meshes: halo sums over ranks -------------------------
+ * A rank that holds part of the mesh (its elements, every node they touch,
+ * Ml / invMl of the whole mesh) sums assembled nodal fields with the ranks
+ * that share its nodes, where the reference calls
+ * mpi_halo_atomic_update_real_arrays / _massEnerMom
+ * (src/lib_sod2d/sources/mod_comms.f90:776-877 with the NCCL transport of
+ * :1049-1102): inside sod_gpu_full_proj_ijk (elem_stab.f90:563-571) and
+ * inside sod_gpu_updateF on the projections and on the residuals
+ * (time_integ_ls.f90:663-667).  The plan has the reference's comms arrays
+ * (HOST, 1-based): ranksToComm(numRanksWithComms), commsMemPosInLoc and
+ * commsMemSize per neighbour, nodesToComm(sum of commsMemSize) as local
+ * node ids, each neighbour's range listing the shared nodes in the same
+ * order on both sides.  send_buf and recv_buf are DEVICE buffers of
+ * 12 * numNodesToComm floats owned by the caller (the reference's
+ * aux_realField_s / aux_realField_r).
+ *
+ * A width-W exchange packs node j of nodesToComm, component k, at
+ * send_buf[j*W + k] on the context's stream, then calls
+ * exchange(user, send_buf, recv_buf, W, stream), which sends, for every
+ * neighbour i, the floats [(commsMemPosInLoc(i)-1)*W, +commsMemSize(i)*W)
+ * of send_buf to rank ranksToComm(i) and receives the same range of
+ * recv_buf from it (mpi_base_comms_real_ncclSendRcv(numArrays)); when it
+ * returns, the transfers are complete or enqueued on `stream`, and a
+ * non-zero return fails the calling entry point.  Each shared node is then
+ * summed over its ranks in ascending rank order, so all ranks hold
+ * bit-identical values (the reference's per-neighbour atomic adds do not
+ * guarantee that for nodes on three or more ranks).  numRanksWithComms = 0
+ * removes the plan. */
+typedef int (*sod_halo_exchange_fn)(void *user, float *send_buf, float *recv_buf, int width, void *stream);
+int sod_gpu_set_halo(sod_gpu_ctx *ctx, int rank, int numRanksWithComms, const int *ranksToComm,
+                     const int *commsMemPosInLoc, const int *commsMemSize, const int *nodesToComm,
+                     float *send_buf, float *recv_buf, sod_halo_exchange_fn exchange, void *user);
+/* mpi_halo_atomic_update_real_arrays(ncomp, field): field(npoin,ncomp)
+ * (device, reference layout) summed over the ranks that share each node. */
+int sod_gpu_halo_update(sod_gpu_ctx *ctx, float *field, int ncomp);
+
 /* ---- element operators (device pointers, FP32, reference layout) ------ */
 
 /* Split-form convective residual.  Replaces full_convec_ijk,

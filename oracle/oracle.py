@@ -480,3 +480,47 @@ def elem_jacobian(porder, nelem, npoin, connec, coord, dNgp, wgp, dtype=np.float
 
 def load_history(path) -> np.ndarray:
     return np.loadtxt(path, ndmin=2)
+
+
+_HALO_CB = {np.float32: C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.POINTER(C.c_float)), C.c_int, C.c_longlong),
+            np.float64: C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.POINTER(C.c_double)), C.c_int, C.c_longlong)}
+_halo_keep = {}
+
+
+def set_halo(fn, dtype=np.float32):
+    """Install fn(list of ncomp numpy views of npoin values) at the oracle's
+    halo points (the reference's mpi_halo_atomic_update_* calls inside
+    full_proj_ijk and updateF); None removes it."""
+    dt = np.dtype(dtype).type
+    suffix = "f32" if dt is np.float32 else "f64"
+    setter = getattr(lib(), f"oracle_set_halo_{suffix}")
+    if fn is None:
+        setter(None, None)
+        _halo_keep.pop(suffix, None)
+        return
+
+    def cb(user, comp, ncomp, npoin):
+        fn([np.ctypeslib.as_array(comp[k], shape=(npoin,)) for k in range(ncomp)])
+
+    c = _HALO_CB[dt](cb)
+    _halo_keep[suffix] = c
+    setter(c, None)
+
+
+def halo_exchange_add(plan, comps, transport):
+    """The reference's halo sum on one rank (mod_comms.f90:467-627 around
+    the transport): fill_sendBuffer_arrays_real packs node i of
+    nodesToComm, array k at (i-1)*W + k; the transport exchanges the
+    neighbour ranges; copy_from_rcvBuffer_arrays_real adds the received
+    values to the local ones, entry by entry in nodesToComm order."""
+    import torch
+    W = len(comps)
+    nodes = plan.nodesToComm.astype(np.int64) - 1
+    send = np.zeros(nodes.size * W, comps[0].dtype)
+    for k, a in enumerate(comps):
+        send[k::W] = a[nodes]
+    recv = np.zeros_like(send)
+    transport.exchange(plan, torch.from_numpy(send), torch.from_numpy(recv), W)
+    for i, p in enumerate(nodes):
+        for k, a in enumerate(comps):
+            a[p] = a[p] + recv[i * W + k]

@@ -134,6 +134,7 @@ struct CompSolver {
       full_diffusion_ijk<R>(m, g, (R)prm.Cp, (R)prm.Prt, rho2, rho2, u2, T2, mu_fluid.data(), mu_e.data(),
                             mu_sgs.data(), Rmass.data(), Rmom.data(), Rener.data(), false, R(-1));
     }
+    halo_update<R>({Rmom.data(), Rmom.data() + N, Rmom.data() + 2 * N, Rmass.data(), Rener.data()}, N);
     lumped_solver<R>(m, g, Rmass.data(), 1);
     lumped_solver<R>(m, g, Rener.data(), 1);
     lumped_solver<R>(m, g, Rmom.data(), 3);
@@ -727,6 +728,14 @@ ORACLE_BOTH(DEF_VELOC)
     compute_vorticity<R>(m, g, u, vorti);                                                              \
     return 0;                                                                                          \
   }
+#define DEF_HALO(R, S)                                                                                 \
+  int oracle_set_halo_##S(void (*fn)(void *, R *const *, int, long long), void *user) {                \
+    HaloHook<R>::fn = fn;                                                                                \
+    HaloHook<R>::user = user;                                                                            \
+    return 0;                                                                                            \
+  }
+
 extern "C" {
+ORACLE_BOTH(DEF_HALO)
 ORACLE_BOTH(DEF_ENTROPY)
 }

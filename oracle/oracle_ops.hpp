@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <initializer_list>
 #include <vector>
 #include <algorithm>
 #include <limits>
@@ -272,6 +273,25 @@ void lumped_solver(const Mesh &m, const Geo<R> &g, R *Rv, int ncomp) {
   }
 }
 
+// ---- halo sum of a partitioned mesh ------------------------------------
+// The points where the reference calls mpi_halo_atomic_update_* on a rank
+// of a partitioned mesh (elem_stab.f90:563-571 for the projections,
+// time_integ_ls.f90:663-667 for the residuals), as a hook: the test that
+// runs the oracle on sub-meshes installs a function that exchanges and adds
+// the neighbours' contributions (mod_comms.f90:467-627); without one the
+// mesh is whole and nothing happens.  comp[k] is component k, npoin values.
+template <class R>
+struct HaloHook {
+  static inline void (*fn)(void *user, R *const *comp, int ncomp, long long npoin) = nullptr;
+  static inline void *user = nullptr;
+};
+template <class R>
+inline void halo_update(std::initializer_list<R *> comps, long long npoin) {
+  if (!HaloHook<R>::fn) return;
+  std::vector<R *> v(comps);
+  HaloHook<R>::fn(HaloHook<R>::user, v.data(), (int)v.size(), npoin);
+}
+
 // ---- full_proj_ijk, src/lib_sod2d/sources/elem_stab.f90:441-586 --------
 // Outputs, each (N,3): ProjMass, ProjEner, ProjMX, ProjMY, ProjMZ.
 template <class R>
@@ -315,6 +335,11 @@ void full_proj_ijk(const Mesh &m, const Geo<R> &g, const R *rho, const R *u, con
   R *dst[15] = {PMX, PMX + N, PMX + 2 * N, PMY, PMY + N, PMY + 2 * N, PMZ, PMZ + N, PMZ + 2 * N,
                 PMass, PMass + N, PMass + 2 * N, PEner, PEner + N, PEner + 2 * N};
   scatter(m, buf, 15, dst, R(1));
+  halo_update<R>({PMX, PMX + N, PMX + 2 * N}, N);
+  halo_update<R>({PMY, PMY + N, PMY + 2 * N}, N);
+  halo_update<R>({PMZ, PMZ + N, PMZ + 2 * N}, N);
+  halo_update<R>({PMass, PMass + N, PMass + 2 * N}, N);
+  halo_update<R>({PEner, PEner + N, PEner + 2 * N}, N);
   lumped_solver(m, g, PMX, 3);
   lumped_solver(m, g, PMY, 3);
   lumped_solver(m, g, PMZ, 3);

@@ -7,6 +7,7 @@
 #include "precond_net.cuh"
 #include "veloc_kernels.cuh"
 #include "imex_kernels.cuh"
+#include "halo.cuh"
 
 #include <cuda_runtime.h>
 
@@ -143,6 +144,17 @@ struct sod_gpu_ctx {
     int cg_iters = 0;
     double cg_res = 0.0;
   } imex;
+  // halo plan of a partitioned mesh (sod_gpu_set_halo)
+  struct Halo {
+    bool on = false;
+    int rank = 0, nsend = 0, nuniq = 0;
+    int *send_node = nullptr;                    // [nsend] local node (0-based) of each buffer position
+    int *uniq_node = nullptr, *ptr = nullptr, *src = nullptr;  // shared nodes, rank-ordered contributions
+    float *send = nullptr, *recv = nullptr;
+    sod_halo_exchange_fn fn = nullptr;
+    void *user = nullptr;
+    std::vector<void *> own;                     // device arrays of the current plan
+  } halo;
 
   MeshDev md() const {
     MeshDev m;
@@ -303,6 +315,39 @@ void gather_proj_aos(sod_gpu_ctx *c) {
   k_gather<12, 12, true><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsA, c->proj12, none, 0, 1);
 }
 
+// Sum the view's components over the ranks that share each node (no-op
+// without a halo plan).
+int halo_sum(sod_gpu_ctx *c, const HaloView &v) {
+  auto &h = c->halo;
+  if (!h.on) return 0;
+  if (h.nsend > 0)
+    k_halo_pack<<<nblk(h.nsend, 256), 256, 0, c->stream>>>(h.nsend, h.send_node, v, h.send);
+  CUDA_TRY(cudaGetLastError());
+  if (h.fn(h.user, h.send, h.recv, v.width, (void *)c->stream) != 0)
+    return fail(SOD_GPU_EINVAL, "halo exchange callback failed");
+  if (h.nuniq > 0)
+    k_halo_sum<<<nblk(h.nuniq, 128), 128, 0, c->stream>>>(h.nuniq, h.uniq_node, h.ptr, h.src, v, h.recv);
+  CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+HaloView halo_proj_view(sod_gpu_ctx *c) {
+  HaloView v{};
+  v.width = 12;
+  v.nstride = 12;
+  for (int k = 0; k < 12; ++k) v.comp[k] = c->proj12 + k;
+  return v;
+}
+
+HaloView halo_res_view(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener) {
+  HaloView v{};
+  const long long N = c->npoin;
+  v.width = 5;
+  v.nstride = 1;
+  v.comp[0] = Rmass; v.comp[1] = Rener; v.comp[2] = Rmom; v.comp[3] = Rmom + N; v.comp[4] = Rmom + 2 * N;
+  return v;
+}
+
 void gather_res(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener, int accumulate, int invml) {
   OutPtrs o{};
   const long long N = c->npoin;
@@ -425,6 +470,7 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
 
 int sod_gpu_finalize(sod_gpu_ctx *ctx) {
   if (!ctx) return 0;
+  for (void *p : ctx->halo.own) cudaFree(p);
   for (void *p : ctx->allocs) cudaFree(p);
   for (void *p : ctx->host_allocs) cudaFreeHost(p);
   delete ctx;
@@ -447,6 +493,98 @@ int sod_gpu_synchronize(sod_gpu_ctx *ctx) {
   if (!ctx) return fail(SOD_GPU_EINVAL, "null context");
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return 0;
+}
+
+int sod_gpu_set_halo(sod_gpu_ctx *c, int rank, int nnb, const int *ranksToComm, const int *commsMemPosInLoc,
+                     const int *commsMemSize, const int *nodesToComm, float *send_buf, float *recv_buf,
+                     sod_halo_exchange_fn exchange, void *user) {
+  if (!c) return fail(SOD_GPU_EINVAL, "null context");
+  auto &h = c->halo;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  for (void *p : h.own) cudaFree(p);
+  h.own.clear();
+  h.on = false;
+  h.nsend = h.nuniq = 0;
+  if (nnb == 0) return 0;
+  if (nnb < 0 || !ranksToComm || !commsMemPosInLoc || !commsMemSize || !nodesToComm || !send_buf || !recv_buf ||
+      !exchange || rank < 0)
+    return fail(SOD_GPU_EINVAL, "bad halo plan argument");
+  // validate the plan: contiguous neighbour ranges, distinct neighbours,
+  // node ids in range, no node twice in one neighbour's range
+  long long nsend = 0;
+  for (int i = 0; i < nnb; ++i) {
+    if (commsMemSize[i] < 0 || commsMemPosInLoc[i] != nsend + 1 || ranksToComm[i] < 0 || ranksToComm[i] == rank)
+      return fail(SOD_GPU_EINVAL, "halo plan: neighbour ranges must be contiguous, 1-based, other ranks");
+    for (int j = 0; j < i; ++j)
+      if (ranksToComm[j] == ranksToComm[i]) return fail(SOD_GPU_EINVAL, "halo plan: neighbour listed twice");
+    nsend += commsMemSize[i];
+  }
+  if (nsend > (1LL << 30)) return fail(SOD_GPU_EINVAL, "halo plan too large");
+  std::vector<int> send_node((size_t)nsend);
+  std::vector<std::vector<std::pair<int, int>>> per_node;
+  std::vector<int> slot_of((size_t)c->npoin, -1);
+  std::vector<int> uniq;
+  for (int i = 0; i < nnb; ++i) {
+    for (long long j = commsMemPosInLoc[i] - 1; j < commsMemPosInLoc[i] - 1 + commsMemSize[i]; ++j) {
+      const int node = nodesToComm[j] - 1;
+      if (node < 0 || node >= c->npoin) return fail(SOD_GPU_EINVAL, "halo plan: node id out of range");
+      send_node[(size_t)j] = node;
+      int &s = slot_of[(size_t)node];
+      if (s < 0) {
+        s = (int)uniq.size();
+        uniq.push_back(node);
+        per_node.push_back({{rank, -1}});
+      }
+      for (auto &pr : per_node[(size_t)s])
+        if (pr.first == ranksToComm[i]) return fail(SOD_GPU_EINVAL, "halo plan: node listed twice for a neighbour");
+      per_node[(size_t)s].push_back({ranksToComm[i], (int)j});
+    }
+  }
+  std::vector<int> ptr(uniq.size() + 1, 0), src;
+  for (size_t u = 0; u < uniq.size(); ++u) {
+    auto &v = per_node[u];
+    std::sort(v.begin(), v.end());
+    for (auto &pr : v) src.push_back(pr.second);
+    ptr[u + 1] = (int)src.size();
+  }
+  auto up = [&](int **d, const std::vector<int> &hv) -> int {
+    size_t b = std::max<size_t>(hv.size(), 1) * sizeof(int);
+    cudaError_t e = cudaMalloc((void **)d, b);
+    if (e != cudaSuccess) return fail(SOD_GPU_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h.own.push_back(*d);
+    if (!hv.empty()) CUDA_TRY(cudaMemcpy(*d, hv.data(), hv.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return 0;
+  };
+  int rc;
+  if ((rc = up(&h.send_node, send_node)) || (rc = up(&h.uniq_node, uniq)) || (rc = up(&h.ptr, ptr)) ||
+      (rc = up(&h.src, src))) {
+    for (void *p : h.own) cudaFree(p);
+    h.own.clear();
+    return rc;
+  }
+  h.rank = rank;
+  h.nsend = (int)nsend;
+  h.nuniq = (int)uniq.size();
+  h.send = send_buf;
+  h.recv = recv_buf;
+  h.fn = exchange;
+  h.user = user;
+  h.on = true;
+  return 0;
+}
+
+int sod_gpu_halo_update(sod_gpu_ctx *c, float *field, int ncomp) {
+  if (!c || !field || ncomp < 1) return fail(SOD_GPU_EINVAL, "bad argument");
+  const long long N = c->npoin;
+  for (int k0 = 0; k0 < ncomp; k0 += HALO_MAX_WIDTH) {
+    HaloView v{};
+    v.width = std::min(HALO_MAX_WIDTH, ncomp - k0);
+    v.nstride = 1;
+    for (int k = 0; k < v.width; ++k) v.comp[k] = field + (k0 + k) * N;
+    int rc = halo_sum(c, v);
+    if (rc) return rc;
+  }
+  return c->finish();
 }
 
 int sod_gpu_lumped_solver(sod_gpu_ctx *c, float *R, int ncomp) {
@@ -489,6 +627,7 @@ int sod_gpu_full_proj_ijk(sod_gpu_ctx *c, const float *rho, const float *u, cons
   // assemble into the node-major 12-wide buffer, then expand to the
   // reference's five (npoin,3) arrays
   gather_proj_aos(c);
+  if ((rc = halo_sum(c, halo_proj_view(c)))) return rc;
   k_unpack_proj<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, c->proj12, ProjMX, ProjMY, ProjMZ, ProjMass,
                                                             ProjEner);
   return c->finish();
@@ -585,11 +724,14 @@ int sod_gpu_updateF(sod_gpu_ctx *c, const float *rho, const float *q, const floa
   int rc = dispatch(c, [&](auto L) {
     L.proj(c, false, rho, q, E);
     gather_proj_aos(c);
+    int hrc = halo_sum(c, halo_proj_view(c));
+    if (hrc) return hrc;
     L.template rhs<MODE_CONV | MODE_DIFF, IN_CONS>(c, A);
     return 0;
   });
   if (rc) return rc;
   gather_res(c, Rmass, Rmom, Rener, 0, 1);
+  if ((rc = halo_sum(c, halo_res_view(c, Rmass, Rmom, Rener)))) return rc;
   if (u_out || pr_out || Tem_out || mu_fluid_out)
     k_eos_out<<<nblk(c->npoin_w, 256), 256, 0, c->stream>>>(c->npoin_w, c->npoin, c->lpoin_w, c->ph, c->phys.Rgas,
                                                             mu_factor, rho, q, E, u_out, pr_out, Tem_out,

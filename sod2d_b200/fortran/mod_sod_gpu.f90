@@ -68,6 +68,19 @@ module mod_sod_gpu
       real(c_float)  :: mu_factor
    end type
 
+   ! The halo exchange a rank hands to sod_gpu_set_halo (c_funloc of a
+   ! bind(C) function of this shape): for every neighbour i, send the floats
+   ! [(commsMemPosInLoc(i)-1)*width, +commsMemSize(i)*width) of send_buf to
+   ! ranksToComm(i) and receive the same range of recv_buf from it, as
+   ! mpi_base_comms_real_ncclSendRcv(width) does; return 0 on success.
+   abstract interface
+      integer(c_int) function sod_halo_exchange_fn(user, send_buf, recv_buf, width, stream) bind(C)
+         import :: c_int, c_ptr
+         type(c_ptr), value :: user, send_buf, recv_buf, stream
+         integer(c_int), value :: width
+      end function
+   end interface
+
    interface
       integer(c_int) function sod_gpu_init(mesh, phys, out) bind(C, name='sod_gpu_init')
          import :: c_int, c_ptr, sod_mesh_t, sod_phys_t
@@ -98,6 +111,19 @@ module mod_sod_gpu
       integer(c_size_t) function sod_gpu_device_bytes(ctx) bind(C, name='sod_gpu_device_bytes')
          import :: c_int, c_ptr, c_size_t
          type(c_ptr), value :: ctx
+      end function
+      integer(c_int) function sod_gpu_set_halo(ctx, rank, numRanksWithComms, ranksToComm, commsMemPosInLoc, &
+         commsMemSize, nodesToComm, send_buf, recv_buf, exchange, user) bind(C, name='sod_gpu_set_halo')
+         import :: c_funptr, c_int, c_ptr
+         type(c_ptr), value :: ctx, send_buf, recv_buf, user
+         integer(c_int), value :: rank, numRanksWithComms
+         integer(c_int), intent(in) :: ranksToComm(*), commsMemPosInLoc(*), commsMemSize(*), nodesToComm(*)
+         type(c_funptr), value :: exchange
+      end function
+      integer(c_int) function sod_gpu_halo_update(ctx, field, ncomp) bind(C, name='sod_gpu_halo_update')
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx, field
+         integer(c_int), value :: ncomp
       end function
       integer(c_int) function sod_gpu_full_convec_ijk(ctx, u, q, rho, pr, E, Rmass, Rmom, Rener, &
          initialze, fact) bind(C, name='sod_gpu_full_convec_ijk')

@@ -18,6 +18,8 @@ _lib = None
 P_I = C.POINTER(C.c_int)
 P_F = C.POINTER(C.c_float)
 VP = C.c_void_p
+# sod_halo_exchange_fn(user, send_buf, recv_buf, width, stream)
+HALO_FN = C.CFUNCTYPE(C.c_int, VP, VP, VP, C.c_int, VP)
 
 
 class SodMesh(C.Structure):
@@ -107,6 +109,8 @@ SIGNATURES = {
                                          C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "sod_gpu_analysis_noalloc": (C.c_int, [C.c_int] * 4 + [VP] * 15 + [C.c_float, C.c_float, VP,
                                                                        C.POINTER(C.c_double)]),
+    "sod_gpu_set_halo": (C.c_int, [VP, C.c_int, C.c_int, P_I, P_I, P_I, P_I, VP, VP, HALO_FN, VP]),
+    "sod_gpu_halo_update": (C.c_int, [VP, VP, C.c_int]),
 }
 
 
@@ -187,7 +191,39 @@ class Context:
             pass
 
     def call(self, name, *args):
-        check(getattr(lib(), name)(self.h, *args), name)
+        rc = getattr(lib(), name)(self.h, *args)
+        err = getattr(self, "_halo", {}).pop("err", None)
+        if rc != 0 and err is not None:
+            raise RuntimeError(f"{name}: halo exchange failed") from err
+        check(rc, name)
+
+    def set_halo(self, plan, transport):
+        """Attach a halo plan (sod2d_b200.partition.HaloPlan) and a transport
+        with exchange(plan, send, recv, width); the send / receive buffers are
+        device tensors of 12 floats per entry of nodesToComm."""
+        import torch
+        n = 12 * max(plan.numNodesToComm, 1)
+        h = dict(send=torch.zeros(n, device="cuda"), recv=torch.zeros(n, device="cuda"), plan=plan)
+        ints = [np.ascontiguousarray(a, np.int32) for a in (plan.ranksToComm, plan.commsMemPosInLoc,
+                                                            plan.commsMemSize, plan.nodesToComm)]
+        if ints[3].size == 0:
+            ints[3] = np.zeros(1, np.int32)
+
+        def cb(user, send_buf, recv_buf, width, stream):
+            try:
+                transport.exchange(plan, h["send"], h["recv"], int(width))
+                return 0
+            except BaseException as e:  # noqa: BLE001 - re-raised by call()
+                h["err"] = e
+                return -1
+
+        h["fn"], h["ints"] = HALO_FN(cb), ints
+        if hasattr(transport, "register"):
+            transport.register(plan.rank, h["send"])
+        self._halo = h
+        self.call("sod_gpu_set_halo", plan.rank, plan.numRanksWithComms, *(a.ctypes.data_as(P_I) for a in ints),
+                  dptr(h["send"]), dptr(h["recv"]), h["fn"], None)
+        return h
 
     @property
     def device_bytes(self) -> int:

@@ -76,6 +76,8 @@ def test_argument_kinds_and_passing_match_the_header():
                 assert attrs.startswith(f"type({ty}), intent("), where
             elif stars == "*" and ty in ("sod_gpu_ctx", "void"):
                 assert attrs == "type(c_ptr), value", where
+            elif ty.endswith("_fn"):  # function-pointer typedef
+                assert attrs == "type(c_funptr), value", where
             elif stars == "*":
                 # device address, or a host output / host array of the C type
                 assert attrs == "type(c_ptr), value" or (attrs.startswith(KIND[ty] + ", intent(")
@@ -95,7 +97,8 @@ def test_host_outputs_are_by_reference():
             "sod_gpu_incomp_analysis": ("out",), "sod_gpu_comp_analysis": ("out",),
             "sod_gpu_analysis_noalloc": ("out",), "sod_gpu_precond_set_params": ("host_params",),
             "sod_gpu_precond_get_params": ("host_params",), "sod_gpu_precond_loss_grad": ("loss", "grad_host"),
-            "sod_gpu_precond_train": ("final_loss",)}
+            "sod_gpu_precond_train": ("final_loss",),
+            "sod_gpu_set_halo": ("ranksToComm", "commsMemPosInLoc", "commsMemSize", "nodesToComm")}
     for name, args in host.items():
         decls = f[name][2]
         for a in args:
