@@ -124,6 +124,27 @@ int sod_gpu_set_halo(sod_gpu_ctx *ctx, int rank, int numRanksWithComms, const in
 /* mpi_halo_atomic_update_real_arrays(ncomp, field): field(npoin,ncomp)
  * (device, reference layout) summed over the ranks that share each node. */
 int sod_gpu_halo_update(sod_gpu_ctx *ctx, float *field, int ncomp);
+/* Global reductions of a partitioned mesh, the reference's MPI_Allreduce
+ * calls of the explicit step: min rho of the entropy viscosity
+ * (mod_entropy_viscosity.f90:161), the CFL time step (mod_time_ops.f90:59)
+ * and the analysis integrals (mod_analysis.f90:39, 134-135, 166).
+ * allreduce(user, buf, count, kind, stream) reduces `count` values of the
+ * DEVICE buffer `buf` in place over all ranks: kind SOD_REDUCE_MIN_F32 /
+ * SOD_REDUCE_MAX_F32 (float) or SOD_REDUCE_SUM_F64 (double); when it
+ * returns the result is in `buf` or enqueued on `stream`.  Every rank of the
+ * plan makes the same calls in the same order.  Setting it (a collective
+ * call) also sums the mesh volume of the analysis over the ranks.  With a
+ * halo plan, sod_gpu_comp_rk_ls_step, sod_gpu_comp_adapt_dt and
+ * sod_gpu_comp_analysis do the halo sums and reductions of rk_4_ls_main;
+ * the entry points whose solves need global dot products
+ * (sod_gpu_conjgrad_pressure, sod_gpu_pressure_solve,
+ * sod_gpu_conjgrad_veloc, sod_gpu_incomp_*, sod_gpu_comp_imex_step) return
+ * SOD_GPU_EINVAL on a context with a halo plan. */
+#define SOD_REDUCE_MIN_F32 0
+#define SOD_REDUCE_MAX_F32 1
+#define SOD_REDUCE_SUM_F64 2
+typedef int (*sod_allreduce_fn)(void *user, void *buf, int count, int kind, void *stream);
+int sod_gpu_set_allreduce(sod_gpu_ctx *ctx, sod_allreduce_fn allreduce, void *user);
 
 /* ---- element operators (device pointers, FP32, reference layout) ------ */
 

@@ -154,6 +154,9 @@ struct sod_gpu_ctx {
     sod_halo_exchange_fn fn = nullptr;
     void *user = nullptr;
     std::vector<void *> own;                     // device arrays of the current plan
+    sod_allreduce_fn reduce = nullptr;           // global reductions (sod_gpu_set_allreduce)
+    void *reduce_user = nullptr;
+    double *vol = nullptr;                       // scratch of the volume sum
   } halo;
 
   MeshDev md() const {
@@ -346,6 +349,22 @@ HaloView halo_res_view(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener) 
   v.nstride = 1;
   v.comp[0] = Rmass; v.comp[1] = Rener; v.comp[2] = Rmom; v.comp[3] = Rmom + N; v.comp[4] = Rmom + 2 * N;
   return v;
+}
+
+// In-place global reduction of a device buffer (no-op without a callback).
+int allreduce(sod_gpu_ctx *c, void *buf, int count, int kind) {
+  auto &h = c->halo;
+  if (!h.reduce) return 0;
+  CUDA_TRY(cudaGetLastError());
+  if (h.reduce(h.reduce_user, buf, count, kind, (void *)c->stream) != 0)
+    return fail(SOD_GPU_EINVAL, "allreduce callback failed");
+  return 0;
+}
+
+// Entry points whose solves need global dot products refuse a partitioned mesh.
+int no_partition(sod_gpu_ctx *c, const char *what) {
+  if (c && c->halo.on) return fail(SOD_GPU_EINVAL, std::string(what) + " is not available with a halo plan");
+  return 0;
 }
 
 void gather_res(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener, int accumulate, int invml) {
@@ -585,6 +604,24 @@ int sod_gpu_halo_update(sod_gpu_ctx *c, float *field, int ncomp) {
     if (rc) return rc;
   }
   return c->finish();
+}
+
+int sod_gpu_set_allreduce(sod_gpu_ctx *c, sod_allreduce_fn fn, void *user) {
+  if (!c) return fail(SOD_GPU_EINVAL, "null context");
+  auto &h = c->halo;
+  h.reduce = fn;
+  h.reduce_user = user;
+  if (!fn) return 0;
+  int rc;
+  if (!h.vol && (rc = c->alloc(&h.vol, 1))) return rc;
+  // mesh volume of the analysis (visc_dissipationRate's volT): sum over ranks
+  double v = (double)c->volT;
+  CUDA_TRY(cudaMemcpyAsync(h.vol, &v, 8, cudaMemcpyHostToDevice, c->stream));
+  if ((rc = allreduce(c, h.vol, 1, SOD_REDUCE_SUM_F64))) return rc;
+  CUDA_TRY(cudaMemcpyAsync(&v, h.vol, 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->volT = (float)v;
+  return 0;
 }
 
 int sod_gpu_lumped_solver(sod_gpu_ctx *c, float *R, int ncomp) {
@@ -977,6 +1014,7 @@ int sod_gpu_full_convec_ijk_incomp(sod_gpu_ctx *c, const float *u, const float *
 int sod_gpu_conjgrad_pressure(sod_gpu_ctx *c, const float *Rp0, float *R, int maxIter, double tol, int *iters,
                               double *res_rel) {
   if (!c || !Rp0 || !R || maxIter < 1) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_conjgrad_pressure")) return prc;
   int rc;
   if ((rc = ensure_diag(c)) || (rc = ensure_cg32(c))) return rc;
   auto &G = c->cg;
@@ -1089,6 +1127,7 @@ extern "C" {
 int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const sod_solve_opts_t *opts,
                            sod_solve_stats_t *stats) {
   if (!c || !b_in || !x || !opts || opts->max_iter < 1 || !(opts->tol > 0)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_pressure_solve")) return prc;
   if (opts->precond != 0 && opts->precond != 1) return fail(SOD_GPU_EINVAL, "precond must be 0 or 1");
   int rc;
   if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c)) || (rc = ensure_cg_loop(c))) return rc;
@@ -1404,23 +1443,27 @@ void launch_stage(sod_gpu_ctx *c, double l1, double li, double gdt, int first) {
 }
 
 // RHS at the current FP32 shadow state into comp.R* (updateF body).
-void comp_updateF(sod_gpu_ctx *c) {
+int comp_updateF(sod_gpu_ctx *c) {
   auto &S = c->comp;
   RhsArgs A{};
   A.rho = S.rho32; A.q = S.q32; A.E = S.E32; A.mu_factor = S.mu_factor;
   A.mue_t = c->mue_t; A.tau_stab = S.tau; A.proj12 = c->proj12;
   A.fact_c = -1.0f; A.fact_d = -1.0f;
-  dispatch(c, [&](auto L) {
+  int rc = dispatch(c, [&](auto L) {
     L.proj(c, false, S.rho32, S.q32, S.E32);
     gather_proj_aos(c);
+    int hrc = halo_sum(c, halo_proj_view(c));
+    if (hrc) return hrc;
     L.template rhs<MODE_CONV | MODE_DIFF, IN_CONS>(c, A);
     return 0;
   });
+  if (rc) return rc;
   gather_res(c, S.Rmass, S.Rmom, S.Rener, 0, 1);
+  return halo_sum(c, halo_res_view(c, S.Rmass, S.Rmom, S.Rener));
 }
 
 // Entropy residual (+ divergence and vorticity when dc) of (feta, eta1, u1[, u2]).
-void comp_entropy_pass(sod_gpu_ctx *c, float *Reta_out, bool dc) {
+int comp_entropy_pass(sod_gpu_ctx *c, float *Reta_out, bool dc) {
   auto &S = c->comp;
   dispatch(c, [&](auto L) {
     using LL = decltype(L);
@@ -1435,13 +1478,25 @@ void comp_entropy_pass(sod_gpu_ctx *c, float *Reta_out, bool dc) {
   });
   k_gather_entropy<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, c->lelpn, c->is_work, Reta_out,
                                                                S.divU, S.vort, dc ? 1 : 0);
+  // halo sums of the lumped entropy residual (time_integ_ls.f90:287, :431),
+  // the divergence and the vorticity (mod_operators.f90:566, :759)
+  HaloView v{};
+  const long long N = c->npoin;
+  v.nstride = 1;
+  v.width = dc ? 5 : 1;
+  v.comp[0] = Reta_out;
+  if (dc) { v.comp[1] = S.divU; v.comp[2] = S.vort; v.comp[3] = S.vort + N; v.comp[4] = S.vort + 2 * N; }
+  return halo_sum(c, v);
 }
 
-void comp_visc(sod_gpu_ctx *c, const float *Reta, const float *rho, const float *u, bool ducros) {
+int comp_visc(sod_gpu_ctx *c, const float *Reta, const float *rho, const float *u, bool ducros) {
   auto &S = c->comp;
   const unsigned init_bits = 0x47C35000u;  // 100000.0f
-  cudaMemcpyAsync(S.bits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream);
+  CUDA_TRY(cudaMemcpyAsync(S.bits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
   k_min_rho<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, S.bits);
+  // the bits of a positive float order like the float: reduce as float
+  int rc = allreduce(c, S.bits, 1, SOD_REDUCE_MIN_F32);
+  if (rc) return rc;
   ViscArgs V{};
   V.Reta = Reta; V.rho = rho; V.u = u; V.csound = S.csound; V.divU = S.divU; V.vort = S.vort; V.Ml = c->Ml;
   V.helem = c->helem; V.helem_l_t = c->helem_l_t; V.min_rho_bits = S.bits;
@@ -1452,6 +1507,7 @@ void comp_visc(sod_gpu_ctx *c, const float *Reta, const float *rho, const float 
     k_visc<LL::P_><<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->md(), V, c->a_of_t, c->mue_t, nullptr);
     return 0;
   });
+  return 0;
 }
 
 }  // namespace
@@ -1483,6 +1539,7 @@ int sod_gpu_smart_visc_spectral_imex(sod_gpu_ctx *c, const float *Reta, const fl
   const unsigned init_bits = 0x47C35000u;  // 100000.0f, the reference's initial minimum
   CUDA_TRY(cudaMemcpyAsync(c->vbits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
   k_min_rho<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, c->vbits);
+  if ((rc = allreduce(c, c->vbits, 1, SOD_REDUCE_MIN_F32))) return rc;
   ViscArgs V{};
   V.Reta = Reta; V.rho = rho; V.u = u; V.csound = csound; V.Ml = c->Ml;
   V.helem = c->helem; V.helem_l_t = c->helem_l_t; V.min_rho_bits = c->vbits;
@@ -1608,9 +1665,10 @@ int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *c, float dt) {
   if (S.first) {
     S.first = false;
     k_feta<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->npoin, c->lpoin_w, S.u1, S.eta1, S.feta);
-    comp_entropy_pass(c, S.Reta1, false);
-    comp_visc(c, S.Reta1, S.rho32, S.u1, false);
-    comp_updateF(c);
+    int rc;
+    if ((rc = comp_entropy_pass(c, S.Reta1, false)) || (rc = comp_visc(c, S.Reta1, S.rho32, S.u1, false)) ||
+        (rc = comp_updateF(c)))
+      return rc;
   }
   const double dtd = (double)dt;
   auto stage = [&](double l1, double li, double g, int first) {
@@ -1622,7 +1680,8 @@ int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *c, float dt) {
   };
   stage(0.0, 0.0, as_rp(S.gam[2][1], S.fp64), 1);
   for (int i = 2; i <= S.stages; ++i) {
-    comp_updateF(c);
+    int rc = comp_updateF(c);
+    if (rc) return rc;
     stage(as_rp(S.lam[i + 1][1], S.fp64), as_rp(S.lam[i + 1][i], S.fp64), as_rp(S.gam[i + 1][i], S.fp64), 0);
   }
   const float gm = c->phys.gamma_gas;
@@ -1632,10 +1691,11 @@ int sod_gpu_comp_rk_ls_step(sod_gpu_ctx *c, float dt) {
   k_thermo_entropy<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->npoin, c->lpoin_w, gm, c->phys.p_inf,
                                                           c->phys.rho_inf, S.rho32, S.pr, S.u1, S.eta1, S.eta2,
                                                           S.feta);
-  comp_entropy_pass(c, S.Reta2, true);
+  int rc = comp_entropy_pass(c, S.Reta2, true);
+  if (rc) return rc;
   k_aux_reta<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->lpoin_w, dt, S.Reta1, S.Reta2, S.eta1, S.eta2,
                                                     S.aux);
-  comp_visc(c, S.aux, S.rho32, S.u2, true);
+  if ((rc = comp_visc(c, S.aux, S.rho32, S.u2, true))) return rc;
   k_sutherland<<<nblk(c->npoin_w, 256), 256, 0, st>>>(c->npoin_w, c->lpoin_w, S.mu_factor, S.Tem, S.mu_fluid);
   return c->finish();
 }
@@ -1793,6 +1853,7 @@ extern "C" {
 int sod_gpu_comp_imex_step(sod_gpu_ctx *c, float dt, int maxIter, double tol) {
   if (!c || !c->comp.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
   if (!(dt > 0.f) || maxIter < 1 || !(tol > 0.0)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_comp_imex_step")) return prc;
   auto &S = c->comp;
   if (S.stages != 3 && S.stages != 4) return fail(SOD_GPU_EINVAL, "the IMEX integrator has 3 or 4 stages");
   if (S.fp64) return fail(SOD_GPU_EINVAL, "the IMEX integrator runs on the FP32 state (fp64_state = 0)");
@@ -1884,6 +1945,8 @@ int sod_gpu_comp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float cfl_diff, float 
                                                             c->mue_t, S.rho32, cfl_conv, cfl_diff, S.bits + 1);
     return 0;
   });
+  int rc = allreduce(c, S.bits + 1, 1, SOD_REDUCE_MIN_F32);
+  if (rc) return rc;
   unsigned b = 0;
   CUDA_TRY(cudaMemcpyAsync(&b, S.bits + 1, 4, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1906,6 +1969,9 @@ int sod_gpu_comp_analysis(sod_gpu_ctx *c, float rho0, double *out) {
   const unsigned zero = 0u;
   CUDA_TRY(cudaMemcpyAsync(S.bits + 2, &zero, 4, cudaMemcpyHostToDevice, c->stream));
   k_max_mach<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, S.machno, S.bits + 2);
+  int rc;
+  if ((rc = allreduce(c, S.sums, 3, SOD_REDUCE_SUM_F64)) || (rc = allreduce(c, S.bits + 2, 1, SOD_REDUCE_MAX_F32)))
+    return rc;
   double sums[3];
   unsigned mb = 0;
   CUDA_TRY(cudaMemcpyAsync(sums, S.sums, 24, cudaMemcpyDeviceToHost, c->stream));
@@ -2523,6 +2589,7 @@ int sod_gpu_full_diff_stab_incomp(sod_gpu_ctx *c, const float *u, const float *m
 int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu_fluid, const float *mu_sgs,
                            const float *Rp0, float *R, int maxIter, double tol, int *iters, double *res_rel) {
   if (!c || !mu_fluid || !Rp0 || !R || maxIter < 1 || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_conjgrad_veloc")) return prc;
   if (!c->helem) return fail(SOD_GPU_EINVAL, "conjgrad_veloc needs helem at init");
   int rc;
   if ((rc = ensure_velo(c))) return rc;
@@ -2581,6 +2648,7 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu
 
 int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
   if (!c || !u || nu < 0) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_incomp_init")) return prc;
   if (!c->helem) return fail(SOD_GPU_EINVAL, "the incompressible step needs helem at init");
   auto &I = c->inc;
   const size_t N = c->npoin;
@@ -2632,6 +2700,7 @@ int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *c, int *iters, double *res_rel) {
 
 int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats) {
   if (!c || !c->inc.ready || !opts || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_incomp_step")) return prc;
   auto &I = c->inc;
   const long long N = c->npoin;
   const int nw = c->npoin_w;
@@ -2724,6 +2793,7 @@ int sod_gpu_incomp_set_pressure(sod_gpu_ctx *c, const double *p) {
 
 int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float *dt) {
   if (!c || !c->inc.ready || !dt || !(cfl_conv > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_incomp_adapt_dt")) return prc;
   auto &I = c->inc;
   const unsigned init_bits = 0x56B5E621u;  // 1e14f, the reference's initial dt_conv
   CUDA_TRY(cudaMemcpyAsync(I.bits, &init_bits, 4, cudaMemcpyHostToDevice, c->stream));
@@ -2743,6 +2813,7 @@ int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float *dt) {
 
 int sod_gpu_incomp_analysis(sod_gpu_ctx *c, double *out) {
   if (!c || !c->inc.ready || !out) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_incomp_analysis")) return prc;
   auto &I = c->inc;
   dispatch(c, [&](auto L) {
     using LL = decltype(L);

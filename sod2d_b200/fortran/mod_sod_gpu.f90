@@ -28,6 +28,9 @@ module mod_sod_gpu
    integer(c_int), parameter :: SOD_GPU_ENONFINITE = -4  ! a reduction returned NaN/Inf
    integer(c_int), parameter :: SOD_GPU_ESTAGNATE = -5   ! an iterative solve stopped making progress
    integer(c_int), parameter :: SOD_NOALLOC_MAX_ELEM = 1048576
+   integer(c_int), parameter :: SOD_REDUCE_MIN_F32 = 0      ! kinds of sod_allreduce_fn
+   integer(c_int), parameter :: SOD_REDUCE_MAX_F32 = 1
+   integer(c_int), parameter :: SOD_REDUCE_SUM_F64 = 2
 
    ! Mesh and geometry (HOST addresses, reference layout), read by sod_gpu_init.
    type, bind(C) :: sod_mesh_t
@@ -73,11 +76,21 @@ module mod_sod_gpu
    ! [(commsMemPosInLoc(i)-1)*width, +commsMemSize(i)*width) of send_buf to
    ! ranksToComm(i) and receive the same range of recv_buf from it, as
    ! mpi_base_comms_real_ncclSendRcv(width) does; return 0 on success.
+   !
+   ! The global reduction a rank hands to sod_gpu_set_allreduce: reduce
+   ! `count` values of the device buffer `buf` in place over all ranks
+   ! (MPI_Allreduce with MPI_MIN / MPI_MAX on reals, MPI_SUM on real(8), by
+   ! `kind`); return 0 on success.
    abstract interface
       integer(c_int) function sod_halo_exchange_fn(user, send_buf, recv_buf, width, stream) bind(C)
          import :: c_int, c_ptr
          type(c_ptr), value :: user, send_buf, recv_buf, stream
          integer(c_int), value :: width
+      end function
+      integer(c_int) function sod_allreduce_fn(user, buf, count, kind, stream) bind(C)
+         import :: c_int, c_ptr
+         type(c_ptr), value :: user, buf, stream
+         integer(c_int), value :: count, kind
       end function
    end interface
 
@@ -124,6 +137,11 @@ module mod_sod_gpu
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx, field
          integer(c_int), value :: ncomp
+      end function
+      integer(c_int) function sod_gpu_set_allreduce(ctx, allreduce, user) bind(C, name='sod_gpu_set_allreduce')
+         import :: c_funptr, c_int, c_ptr
+         type(c_ptr), value :: ctx, user
+         type(c_funptr), value :: allreduce
       end function
       integer(c_int) function sod_gpu_full_convec_ijk(ctx, u, q, rho, pr, E, Rmass, Rmom, Rener, &
          initialze, fact) bind(C, name='sod_gpu_full_convec_ijk')

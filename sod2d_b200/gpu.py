@@ -20,6 +20,9 @@ P_F = C.POINTER(C.c_float)
 VP = C.c_void_p
 # sod_halo_exchange_fn(user, send_buf, recv_buf, width, stream)
 HALO_FN = C.CFUNCTYPE(C.c_int, VP, VP, VP, C.c_int, VP)
+# sod_allreduce_fn(user, buf, count, kind, stream)
+REDUCE_FN = C.CFUNCTYPE(C.c_int, VP, VP, C.c_int, C.c_int, VP)
+REDUCE_MIN_F32, REDUCE_MAX_F32, REDUCE_SUM_F64 = 0, 1, 2
 
 
 class SodMesh(C.Structure):
@@ -111,6 +114,7 @@ SIGNATURES = {
                                                                        C.POINTER(C.c_double)]),
     "sod_gpu_set_halo": (C.c_int, [VP, C.c_int, C.c_int, P_I, P_I, P_I, P_I, VP, VP, HALO_FN, VP]),
     "sod_gpu_halo_update": (C.c_int, [VP, VP, C.c_int]),
+    "sod_gpu_set_allreduce": (C.c_int, [VP, REDUCE_FN, VP]),
 }
 
 
@@ -137,8 +141,25 @@ def check(rc, what=""):
         raise RuntimeError(f"{what} failed ({rc}): {lib().sod_gpu_last_error().decode()}")
 
 
+def last_error() -> str:
+    """sod_gpu_last_error() of the calling thread."""
+    return lib().sod_gpu_last_error().decode()
+
+
 def _hp(a):
     return None if a is None else a.ctypes.data_as(VP)
+
+
+class _CudaBuffer:
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def device_view(ptr, count, typestr="<f4"):
+    """Zero-copy torch view of `count` elements of device memory at ptr."""
+    import torch
+    return torch.as_tensor(_CudaBuffer(int(ptr), count, typestr), device="cuda")
 
 
 def dptr(t):
@@ -225,6 +246,25 @@ class Context:
                   dptr(h["send"]), dptr(h["recv"]), h["fn"], None)
         return h
 
+    def set_allreduce(self, transport, rank: int):
+        """Global reductions through transport.allreduce(rank, tensor, kind)
+        (a collective call: every rank sets it)."""
+        import torch
+        dtypes = {REDUCE_MIN_F32: (torch.float32, "<f4"), REDUCE_MAX_F32: (torch.float32, "<f4"),
+                  REDUCE_SUM_F64: (torch.float64, "<f8")}
+        h = self.__dict__.setdefault("_halo", {})
+
+        def cb(user, buf, count, kind, stream):
+            try:
+                transport.allreduce(rank, device_view(buf, int(count), dtypes[int(kind)][1]), int(kind))
+                return 0
+            except BaseException as e:  # noqa: BLE001 - re-raised by call()
+                h["err"] = e
+                return -1
+
+        h["reduce_fn"] = REDUCE_FN(cb)
+        self.call("sod_gpu_set_allreduce", h["reduce_fn"], None)
+
     @property
     def device_bytes(self) -> int:
         return int(lib().sod_gpu_device_bytes(self.h))
@@ -238,14 +278,27 @@ class CompSolver:
     (time_integ_imex.f90; the implicit solve's maxIter / tol)."""
 
     def __init__(self, mesh, ic, stages=4, rk_n=1, fp64_state=True, cfl_conv=0.5, cfl_diff=0.5, imex=False,
-                 imex_maxiter=200, imex_tol=1e-3):
+                 imex_maxiter=200, imex_tol=1e-3, partition=None):
+        """partition = (part, transport): run the rank `part`
+        (sod2d_b200.partition.Part of `mesh`) with its halo sums and global
+        reductions through transport (a collective constructor)."""
         import torch
         self.torch = torch
+        npoin = mesh.npoin
+        if partition is not None:
+            part, transport = partition
+            mesh = part.mesh
+            loc = lambda a: np.asarray(a).reshape(-1, npoin)[:, part.nodes].reshape(-1)
+        else:
+            loc = lambda a: a
         self.ctx = Context(mesh, phys_from_ic(ic))
+        if partition is not None:
+            self.ctx.set_halo(part.plan, transport)
+            self.ctx.set_allreduce(transport, part.rank)
         self.mesh, self.ic = mesh, ic
         self.cfl = (cfl_conv, cfl_diff)
         self.imex = (imex_maxiter, imex_tol) if imex else None
-        dv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        dv = lambda a: torch.from_numpy(np.ascontiguousarray(loc(a))).cuda()
         self._init = [dv(a) for a in (ic.rho, ic.u, ic.q, ic.pr, ic.E, ic.Tem, ic.csound, ic.machno, ic.eta)]
         cfg = RkCfg(stages, rk_n, int(fp64_state), ic.mu_factor)
         self.ctx.call("sod_gpu_comp_init_state", C.byref(cfg), *(dptr(t) for t in self._init))

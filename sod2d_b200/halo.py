@@ -16,6 +16,10 @@ ranks in ascending rank order.
   device-to-device copy between the parts' buffers; the threads meet at a
   barrier bounded by a timeout before and after the copies.  No kernel
   waits on another.
+
+Both also provide allreduce(rank, tensor, kind) for the global reductions
+of the explicit step (min / max of float32, sum of float64), the
+reference's MPI_Allreduce calls.
 """
 from __future__ import annotations
 
@@ -32,6 +36,10 @@ class DistHaloTransport:
 
     def _peer(self, r: int) -> int:
         return r if self.group is None else self.dist.get_global_rank(self.group, r)
+
+    def allreduce(self, rank: int, t, kind: int) -> None:
+        ops = (self.dist.ReduceOp.MIN, self.dist.ReduceOp.MAX, self.dist.ReduceOp.SUM)
+        self.dist.all_reduce(t, op=ops[kind], group=self.group)
 
     def exchange(self, plan: HaloPlan, send, recv, width: int) -> None:
         dist = self.dist
@@ -50,10 +58,26 @@ class LocalHaloGroup:
     def __init__(self, plans: list[HaloPlan], timeout: float = 120.0):
         self.plans = {p.rank: p for p in plans}
         self.send = {}
+        self.red = {}
         self.barrier = threading.Barrier(len(plans), timeout=timeout)
 
     def register(self, rank: int, send) -> None:
         self.send[rank] = send
+
+    def allreduce(self, rank: int, t, kind: int) -> None:
+        """min (0), max (1) or sum (2) over the parts, combined in ascending
+        rank order so every part gets the same bits."""
+        import torch
+        self._sync(t)
+        self.red[rank] = t.clone()
+        self.barrier.wait()  # every part has posted its value
+        vals = [self.red[r] for r in sorted(self.red)]
+        acc = vals[0].clone()
+        for v in vals[1:]:
+            acc = torch.minimum(acc, v) if kind == 0 else (torch.maximum(acc, v) if kind == 1 else acc + v)
+        t.copy_(acc)
+        self._sync(t)
+        self.barrier.wait()  # every part has read the others' values
 
     def _sync(self, t) -> None:
         if t.is_cuda:

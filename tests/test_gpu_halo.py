@@ -136,3 +136,114 @@ def test_partitioned_updateF_matches_whole_mesh(gpu, porder, grid):
                 assert val.setdefault(node, bits) == bits, (name, node)
     for c in ctxs:
         c.close()
+
+
+def test_bad_plans_and_failing_exchange(gpu):
+    """sod_gpu_set_halo rejects plans the reference's comms arrays cannot
+    describe (SOD_GPU_EINVAL, checked on the host before any device work),
+    and a transport that fails makes the calling entry point fail with the
+    transport's error, leaving the context usable."""
+    m = host.periodic_cube(3, 4, seed=75)
+    parts = partition.split(m, partition.partition_elements(m, (1, 1, 2)))
+    p = parts[0]
+    ctx = gpu.Context(p.mesh, gpu.default_phys())
+    lib = gpu.lib()
+    buf = torch.zeros(12 * max(p.plan.numNodesToComm, 1), device="cuda")
+    noop = gpu.HALO_FN(lambda *a: 0)
+    ip = lambda a: np.ascontiguousarray(a, np.int32)
+
+    def set_plan(rank, nbs, pos, size, nodes):
+        arrs = [ip(nbs), ip(pos), ip(size), ip(nodes if len(nodes) else [1])]
+        return lib.sod_gpu_set_halo(ctx.h, rank, len(nbs), *(a.ctypes.data_as(gpu.P_I) for a in arrs),
+                                    gpu.dptr(buf), gpu.dptr(buf), noop, None)
+
+    nodes = p.plan.nodesToComm
+    n = nodes.size
+    assert set_plan(0, [1], [1], [n], nodes) == 0
+    assert set_plan(0, [0], [1], [n], nodes) == -1                       # own rank as neighbour
+    assert set_plan(0, [1], [2], [n], nodes) == -1                       # range not starting at 1
+    assert set_plan(0, [1, 1], [1, 2], [1, n - 1], nodes) == -1          # neighbour twice
+    bad = nodes.copy(); bad[0] = p.mesh.npoin + 1
+    assert set_plan(0, [1], [1], [n], bad) == -1                         # node id out of range
+    dup = nodes.copy(); dup[1] = dup[0]
+    assert set_plan(0, [1], [1], [n], dup) == -1                         # node twice for one neighbour
+    assert set_plan(0, [], [], [], []) == 0                              # removes the plan
+
+    class Failing:
+        def exchange(self, plan, send, recv, width):
+            raise ConnectionError("peer went away")
+
+    ctx.set_halo(p.plan, Failing())
+    f = torch.ones(p.mesh.npoin, device="cuda")
+    with pytest.raises(RuntimeError) as ei:
+        ctx.call("sod_gpu_halo_update", gpu.dptr(f), 1)
+    assert isinstance(ei.value.__cause__, ConnectionError)
+    assert "halo exchange" in gpu.last_error()
+    # still usable without the plan
+    assert set_plan(0, [], [], [], []) == 0
+    ctx.call("sod_gpu_halo_update", gpu.dptr(f), 1)
+    assert float(f.sum()) == p.mesh.npoin
+    ctx.close()
+
+
+@pytest.mark.parametrize("porder,grid,stages", [(3, (2, 1, 2), 4), (4, (2, 2, 2), 5)])
+def test_partitioned_rk_time_loop_matches_whole_mesh(gpu, porder, grid, stages):
+    """rk_4_ls_main on a partitioned mesh: every part runs sod_gpu_comp_rk_ls_step
+    with the halo sums of the RHS, the entropy residual, the divergence and
+    the vorticity, and the global min rho / dt / analysis reductions.  The
+    parts agree on every dt and analysis row bit for bit; those rows and
+    the final state match the whole-mesh GPU run to 1e-5 (the reference's
+    TGV at Ma 1.25, entropy viscosity and LPS on)."""
+    m = host.periodic_cube(porder, 4, jitter=0.05, seed=76, elem_shuffle=True, ordering=1)
+    ic = host.tgv_comp_init(m, Ma=1.25)
+    nsteps = 8
+    whole = gpu.CompSolver(m, ic, stages=stages)
+    hw = whole.run(nsteps, log_first=1, log_step=1)
+    sw = whole.state()
+    whole.close()
+
+    parts = partition.split(m, partition.partition_elements(m, grid))
+    group = LocalHaloGroup([p.plan for p in parts], timeout=120.0)
+    solvers = group.run([lambda p=p: gpu.CompSolver(m, ic, stages=stages, partition=(p, group)) for p in parts])
+    hists = group.run([lambda s=s: s.run(nsteps, log_first=1, log_step=1) for s in solvers])
+    states = [s.state() for s in solvers]
+    for h in hists[1:]:
+        assert np.array_equal(h, hists[0])
+    hp = hists[0]
+    assert hp.shape == hw.shape
+    # time, EK, eps_S, eps_D, eps_T, max Mach: dt is a minimum over the state,
+    # so it follows the state's rounding-level differences (different
+    # summation orders of the halo sums)
+    rel = np.abs(hp - hw) / np.maximum(np.abs(hw), 1e-30)
+    print(f"P={porder} {len(parts)} parts: max relative difference per column {rel.max(axis=0)}")
+    assert rel.max() < 1e-5
+    N, n = m.npoin, m.nnode
+    for p, st in zip(parts, states):
+        for key, k in (("rho", 1), ("q", 3), ("E", 1)):
+            ref = sw[key].reshape(k, N)[:, p.nodes].astype(np.float64)
+            err = np.linalg.norm(st[key].reshape(k, -1) - ref) / np.linalg.norm(ref)
+            assert err < 1e-5, (p.rank, key, err)
+        mref = sw["mu_e"].reshape(n, -1)[:, p.elems].astype(np.float64)
+        err = np.linalg.norm(st["mu_e"].reshape(n, -1) - mref) / max(np.linalg.norm(mref), 1e-30)
+        assert err < 1e-4, (p.rank, "mu_e", err)
+    for s in solvers:
+        s.close()
+
+
+def test_partition_refuses_global_solves(gpu):
+    """Entry points whose solves take global dot products refuse a context
+    with a halo plan instead of returning a rank-local answer."""
+    m = host.periodic_cube(3, 4, seed=77)
+    parts = partition.split(m, partition.partition_elements(m, (1, 1, 2)))
+    p = parts[0]
+    ctx = gpu.Context(p.mesh, gpu.default_phys())
+    group = LocalHaloGroup([p.plan], timeout=10.0)  # never exchanges here
+    ctx.set_halo(p.plan, group)
+    x = torch.zeros(p.mesh.npoin, device="cuda")
+    it, res = C.c_int(), C.c_double()
+    with pytest.raises(RuntimeError, match="halo plan"):
+        ctx.call("sod_gpu_conjgrad_pressure", gpu.dptr(x), gpu.dptr(x), 10, 1e-8, C.byref(it), C.byref(res))
+    u = torch.zeros(3 * p.mesh.npoin, device="cuda")
+    with pytest.raises(RuntimeError, match="halo plan"):
+        ctx.call("sod_gpu_incomp_init", gpu.dptr(u), 1e-3)
+    ctx.close()
