@@ -524,3 +524,20 @@ def halo_exchange_add(plan, comps, transport):
     for i, p in enumerate(nodes):
         for k, a in enumerate(comps):
             a[p] = a[p] + recv[i * W + k]
+
+
+_REDUCE_CB = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_int)
+
+
+def set_reduce(fn):
+    """Install fn(values: float64 numpy view, kind) at the oracle's global
+    reductions (the reference's MPI_Allreduce calls: kind 0 min, 1 max,
+    2 sum, in place); None removes it."""
+    setter = lib().oracle_set_reduce
+    if fn is None:
+        setter(None, None)
+        _halo_keep.pop("reduce", None)
+        return
+    c = _REDUCE_CB(lambda user, vals, count, kind: fn(np.ctypeslib.as_array(vals, shape=(count,)), kind))
+    _halo_keep["reduce"] = c
+    setter(c, None)

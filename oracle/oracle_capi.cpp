@@ -170,6 +170,7 @@ struct CompSolver {
         for (int d = 0; d < 3; ++d) f_eta[p + N * d] = u1[p + N * d] * eta1[p];
       }
       generic_scalar_convec_ijk<R>(m, g, f_eta.data(), eta1, u1, Reta.data(), true, R(1));
+      halo_update<R>({Reta.data()}, N);  // time_integ_ls.f90:287
       lumped_solver<R>(m, g, Reta.data(), 1);
       smart_visc_spectral_imex<R>(m, g, Reta.data(), rho1, u1, csound.data(), mu_e.data());
       if (!prm.first_mue) std::fill(mu_e.begin(), mu_e.end(), R(0));
@@ -198,6 +199,7 @@ struct CompSolver {
     thermo_entropy<R>(m, gm, (R)prm.p_inf, (R)prm.rho_inf, rho2, pr2, u1, eta.data(), f_eta.data());
     R *Reta1 = Reta.data(), *Reta2 = Reta.data() + N;
     generic_scalar_convec_ijk<R>(m, g, f_eta.data(), eta1, u1, Reta2, true, R(1));
+    halo_update<R>({Reta2}, N);  // time_integ_ls.f90:431
     lumped_solver<R>(m, g, Reta2, 1);
     for (int t = 0; t < m.npoin_w; ++t) {
       long long p = m.lpoin_w[t] - 1;
@@ -353,6 +355,9 @@ struct CompSolver {
     visc_dissipationRate<R>(m, g, (R)prm.rho_inf, mu_fluid.data(), mu_e.data(), u2, g.volT, &eS, &eD, &eT);
     R mx = 0;
     for (int t = 0; t < m.npoin_w; ++t) mx = std::max(mx, machno[m.lpoin_w[t] - 1]);
+    double mxd = (double)mx;
+    reduce_all(&mxd, 1, 1);  // MPI_Allreduce MAX, mod_analysis.f90:166
+    mx = (R)mxd;
     row[0] = (double)(R)time; row[1] = (double)(R)EK; row[2] = eS; row[3] = eD; row[4] = eT; row[5] = (double)mx;
   }
 
@@ -728,6 +733,12 @@ ORACLE_BOTH(DEF_VELOC)
     compute_vorticity<R>(m, g, u, vorti);                                                              \
     return 0;                                                                                          \
   }
+extern "C" int oracle_set_reduce(void (*fn)(void *, double *, int, int), void *user) {
+  ReduceHook::fn = fn;
+  ReduceHook::user = user;
+  return 0;
+}
+
 #define DEF_HALO(R, S)                                                                                 \
   int oracle_set_halo_##S(void (*fn)(void *, R *const *, int, long long), void *user) {                \
     HaloHook<R>::fn = fn;                                                                                \

@@ -292,6 +292,23 @@ inline void halo_update(std::initializer_list<R *> comps, long long npoin) {
   HaloHook<R>::fn(HaloHook<R>::user, v.data(), (int)v.size(), npoin);
 }
 
+// The reference's MPI_Allreduce calls of the explicit step, as a hook of the
+// same kind: vals reduced in place over the ranks, kind 0 min, 1 max,
+// 2 sum.  Without one the mesh is whole and nothing happens.
+struct ReduceHook {
+  static inline void (*fn)(void *user, double *vals, int count, int kind) = nullptr;
+  static inline void *user = nullptr;
+};
+inline void reduce_all(double *vals, int count, int kind) {
+  if (ReduceHook::fn) ReduceHook::fn(ReduceHook::user, vals, count, kind);
+}
+template <class R>
+inline R reduce_min(R v) {
+  double d = (double)v;
+  reduce_all(&d, 1, 0);
+  return (R)d;
+}
+
 // ---- full_proj_ijk, src/lib_sod2d/sources/elem_stab.f90:441-586 --------
 // Outputs, each (N,3): ProjMass, ProjEner, ProjMX, ProjMY, ProjMZ.
 template <class R>
@@ -556,7 +573,7 @@ void smart_visc_spectral_imex(const Mesh &m, const Geo<R> &g, const R *Reta, con
   const long long N = m.npoin, NE = m.nelem;
   R maxRl = R(100000.0);
   for (int t = 0; t < m.npoin_w; ++t) maxRl = std::min(maxRl, rho[m.lpoin_w[t] - 1]);
-  R norm = maxRl;
+  R norm = reduce_min(maxRl);  // MPI_Allreduce MIN, mod_entropy_viscosity.f90:161
   Idx ix(m);
   for (long long e = 0; e < NE; ++e) {
     R betae = 0;
@@ -629,6 +646,7 @@ void eval_divergence(const Mesh &m, const Geo<R> &g, const R *u, R *Rdiv) {
   }
   R *dst[1] = {Rdiv};
   scatter(m, buf, 1, dst, R(1));
+  halo_update<R>({Rdiv}, N);  // mod_operators.f90:566
 }
 
 // ---- compute_vorticity, mod_operators.f90:684-775 (makeConti = true) ---
@@ -678,6 +696,7 @@ void compute_vorticity(const Mesh &m, const Geo<R> &g, const R *u, R *curlU) {
         for (int j = 0; j < 3; ++j)
           for (int k = 0; k < 3; ++k) curlU[p + N * i] = curlU[p + N * i] + b[t++];
     }
+  halo_update<R>({curlU, curlU + N, curlU + 2 * N}, N);  // mod_operators.f90:759
   for (int t = 0; t < m.npoin_w; ++t) {
     int p = m.lpoin_w[t] - 1;
     for (int d = 0; d < 3; ++d) curlU[p + N * d] = curlU[p + N * d] / R(m.lelpn[p]);
@@ -713,7 +732,7 @@ R adapt_dt_cfl(const Mesh &m, const Geo<R> &g, const R *u, const R *csound, R cf
     dt_diff = std::min(dt_diff, aux4);
     dt_l = std::min(dt_conv, dt_diff);
   }
-  return dt_l;
+  return reduce_min(dt_l);  // MPI_Allreduce MIN, mod_time_ops.f90:59
 }
 
 // ---- volAvg_EK, src/lib_sod2d/sources/mod_analysis.f90:10-44 -----------
@@ -733,6 +752,7 @@ double volAvg_EK(const Mesh &m, const Geo<R> &g, R rho0, const R *rho, const R *
       }
     EK += (double)R1;
   }
+  reduce_all(&EK, 1, 2);  // MPI_Allreduce SUM, mod_analysis.f90:39
   R twopi = R(2.0) * R(3.14159f);
   EK = EK / (double)(rho0 * std::pow(twopi, R(3.0)));
   return EK;
@@ -784,6 +804,10 @@ void visc_dissipationRate(const Mesh &m, const Geo<R> &g, R rho0, const R *mu_fl
   }
   double S = 0, D = 0;
   for (long long e = 0; e < NE; ++e) { S += s1[e]; D += s2[e]; }
+  double SD[2] = {S, D};
+  reduce_all(SD, 2, 2);  // MPI_Allreduce SUM, mod_analysis.f90:134-135
+  S = SD[0];
+  D = SD[1];
   R alpha = R(1.0) / (rho0 * volT);
   S = S * (double)alpha;
   D = (double)(4.0f / 3.0f) * D * (double)alpha;  // default-real literal 4.0/3.0
