@@ -194,8 +194,8 @@ k_vec_elem(MeshDev m, const float *__restrict__ x, const float *__restrict__ u, 
 }
 
 // ---- CG vector kernels (FP64 reductions, deterministic) ---------------
-// Block partial sums of up to 3 dot products over working nodes; a second
-// single-block kernel sums the partials in a fixed order.
+// Dot products over working nodes with FP64 accumulation, summed in a
+// fixed order (deterministic).
 constexpr int DOT_BLOCKS = 592;  // 4 blocks per SM on 148 SMs
 constexpr int DOT_THREADS = 256;
 
@@ -207,10 +207,32 @@ struct DotArgs {
   const V *c[ND];
 };
 
+// Single-block sum of DOT_BLOCKS partials per value, in a fixed order.
+__global__ void k_dot_final(int nd, const double *__restrict__ part, double *__restrict__ out) {
+  __shared__ double sh[1024];
+  for (int d = 0; d < nd; ++d) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < DOT_BLOCKS; b += blockDim.x) s += part[d * DOT_BLOCKS + b];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[d] = sh[0];
+    __syncthreads();
+  }
+}
+
+// ND dot products in one launch: each block reduces its grid-stride share
+// in a fixed order and stores a partial; the last block to take the ticket
+// adds the partials in block order (deterministic) and resets the ticket.
 template <class V, int ND>
-__global__ void k_dot_partial(int npoin_w, const int *__restrict__ lpoin_w, DotArgs<V, ND> A,
-                              double *__restrict__ part) {
+__global__ void __launch_bounds__(DOT_THREADS) k_dot(int npoin_w, const int *__restrict__ lpoin_w,
+                                                     DotArgs<V, ND> A, double *__restrict__ part,
+                                                     unsigned *__restrict__ ticket, double *__restrict__ out) {
   __shared__ double sh[ND][DOT_THREADS];
+  __shared__ bool last;
   double s[ND];
 #pragma unroll
   for (int d = 0; d < ND; ++d) s[d] = 0.0;
@@ -231,24 +253,32 @@ __global__ void k_dot_partial(int npoin_w, const int *__restrict__ lpoin_w, DotA
       for (int d = 0; d < ND; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
 #pragma unroll
-    for (int d = 0; d < ND; ++d) part[d * DOT_BLOCKS + blockIdx.x] = sh[d][0];
-}
-
-__global__ void k_dot_final(int nd, const double *__restrict__ part, double *__restrict__ out) {
-  __shared__ double sh[1024];
-  for (int d = 0; d < nd; ++d) {
-    double s = 0.0;
-    for (int b = threadIdx.x; b < DOT_BLOCKS; b += blockDim.x) s += part[d * DOT_BLOCKS + b];
-    sh[threadIdx.x] = s;
+    for (int d = 0; d < ND; ++d) part[d * gridDim.x + blockIdx.x] = sh[d][0];
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    double v = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) v += __ldcg(part + d * gridDim.x + b);
+    sh[d][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) sh[d][threadIdx.x] += sh[d][threadIdx.x + w];
     __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[d] = sh[0];
-    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int d = 0; d < ND; ++d) out[d] = sh[d][0];
+    *ticket = 0u;
   }
 }
 

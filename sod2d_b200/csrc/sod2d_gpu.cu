@@ -78,6 +78,7 @@ struct sod_gpu_ctx {
     CgScal *S = nullptr, *S_h = nullptr;                        // device-resident CG scalars (+ pinned host copy)
     double *hist = nullptr, *hist_h = nullptr;                  // ||r||^2 per iteration (ring)
     unsigned *ticket = nullptr;                                 // grid-sum ticket
+    unsigned *dticket = nullptr;                                // ticket of k_dot
     double *gpart = nullptr;                                    // grid-sum block partials
   } cg;
   // learned preconditioner
@@ -459,6 +460,15 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
     sod_gpu_finalize(c);
     return rc;
   }
+  if ((rc = c->alloc(&c->cg.dticket, 1)) || (rc = c->alloc(&c->cg.part, (size_t)8 * DOT_BLOCKS)) ||
+      (rc = c->alloc(&c->cg.dots, 16))) {
+    sod_gpu_finalize(c);
+    return rc;
+  }
+  if (cudaMemset(c->cg.dticket, 0, sizeof(unsigned)) != cudaSuccess) {
+    sod_gpu_finalize(c);
+    return fail(SOD_GPU_ECUDA, "cudaMemset of the dot ticket failed");
+  }
   if (mesh->helem && (rc = c->upload(&c->helem, mesh->helem, (size_t)E))) { sod_gpu_finalize(c); return rc; }
   if (mesh->lelpn && (rc = c->upload(&c->lelpn, mesh->lelpn, (size_t)NP))) { sod_gpu_finalize(c); return rc; }
   if (mesh->helem_l) {
@@ -839,8 +849,7 @@ void lap(sod_gpu_ctx *c, const V *p, V *out) {
 
 template <class V, int ND>
 void dots(sod_gpu_ctx *c, DotArgs<V, ND> A, double *out) {
-  k_dot_partial<V, ND><<<DOT_BLOCKS, DOT_THREADS, 0, c->stream>>>(c->npoin_w, c->lpoin_w, A, c->cg.part);
-  k_dot_final<<<1, 1024, 0, c->stream>>>(ND, c->cg.part, out);
+  k_dot<V, ND><<<DOT_BLOCKS, DOT_THREADS, 0, c->stream>>>(c->npoin_w, c->lpoin_w, A, c->cg.part, c->cg.dticket, out);
 }
 
 int ensure_diag(sod_gpu_ctx *c) {
