@@ -892,13 +892,14 @@ int ensure_cg64(sod_gpu_ctx *c) {
 constexpr int CG_HIST = 1024;
 
 int num_sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
+  // initialised once, thread-safely (contexts may be driven from several host threads)
+  static const int n = [] {
+    int dev = 0, v = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
-      n = 148;
-  }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1)
+      v = 148;
+    return v;
+  }();
   return n;
 }
 
