@@ -134,12 +134,15 @@ int sod_gpu_halo_update(sod_gpu_ctx *ctx, float *field, int ncomp);
  * returns the result is in `buf` or enqueued on `stream`.  Every rank of the
  * plan makes the same calls in the same order.  Setting it (a collective
  * call) also sums the mesh volume of the analysis over the ranks.  With a
- * halo plan, sod_gpu_comp_rk_ls_step, sod_gpu_comp_adapt_dt and
- * sod_gpu_comp_analysis do the halo sums and reductions of rk_4_ls_main;
- * the entry points whose solves need global dot products
- * (sod_gpu_conjgrad_pressure, sod_gpu_pressure_solve,
- * sod_gpu_conjgrad_veloc, sod_gpu_incomp_*, sod_gpu_comp_imex_step) return
- * SOD_GPU_EINVAL on a context with a halo plan. */
+ * halo plan, sod_gpu_comp_rk_ls_step, sod_gpu_comp_imex_step,
+ * sod_gpu_comp_adapt_dt and sod_gpu_comp_analysis do the halo sums and
+ * reductions of rk_4_ls_main and imex_main; the IMEX solve's dot products
+ * run over the working nodes this rank owns (a shared node belongs to the
+ * lowest rank holding it; the reference's lpoin_o) and are summed over the
+ * ranks.  The incompressible entry points whose solves need global dot
+ * products (sod_gpu_conjgrad_pressure, sod_gpu_pressure_solve,
+ * sod_gpu_conjgrad_veloc, sod_gpu_incomp_*) return SOD_GPU_EINVAL on a
+ * context with a halo plan. */
 #define SOD_REDUCE_MIN_F32 0
 #define SOD_REDUCE_MAX_F32 1
 #define SOD_REDUCE_SUM_F64 2

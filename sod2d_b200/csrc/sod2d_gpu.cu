@@ -155,6 +155,8 @@ struct sod_gpu_ctx {
     sod_halo_exchange_fn fn = nullptr;
     void *user = nullptr;
     std::vector<void *> own;                     // device arrays of the current plan
+    int npoin_o = 0;                             // working nodes this rank owns (dot products):
+    int *lpoin_o = nullptr;                      //   shared nodes belong to the lowest rank holding them
     sod_allreduce_fn reduce = nullptr;           // global reductions (sod_gpu_set_allreduce)
     void *reduce_user = nullptr;
     double *vol = nullptr;                       // scratch of the volume sum
@@ -584,9 +586,19 @@ int sod_gpu_set_halo(sod_gpu_ctx *c, int rank, int nnb, const int *ranksToComm, 
     if (!hv.empty()) CUDA_TRY(cudaMemcpy(*d, hv.data(), hv.size() * sizeof(int), cudaMemcpyHostToDevice));
     return 0;
   };
+  // owned working nodes (the reference's lpoin_o of its dot products): a
+  // shared node belongs to the lowest rank that holds it
+  std::vector<int> lw((size_t)c->npoin_w), owned;
+  CUDA_TRY(cudaMemcpy(lw.data(), c->lpoin_w, lw.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  owned.reserve(lw.size());
+  for (int p : lw) {
+    const int s = slot_of[(size_t)p];
+    if (s >= 0 && per_node[(size_t)s].front().first < rank) continue;  // sorted by rank: front is the lowest
+    owned.push_back(p);
+  }
   int rc;
   if ((rc = up(&h.send_node, send_node)) || (rc = up(&h.uniq_node, uniq)) || (rc = up(&h.ptr, ptr)) ||
-      (rc = up(&h.src, src))) {
+      (rc = up(&h.src, src)) || (rc = up(&h.lpoin_o, owned))) {
     for (void *p : h.own) cudaFree(p);
     h.own.clear();
     return rc;
@@ -594,6 +606,7 @@ int sod_gpu_set_halo(sod_gpu_ctx *c, int rank, int nnb, const int *ranksToComm, 
   h.rank = rank;
   h.nsend = (int)nsend;
   h.nuniq = (int)uniq.size();
+  h.npoin_o = (int)owned.size();
   h.send = send_buf;
   h.recv = recv_buf;
   h.fn = exchange;
@@ -847,9 +860,14 @@ void lap(sod_gpu_ctx *c, const V *p, V *out) {
   k_gather1<V><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), (const V *)c->slotsB, out, 0);
 }
 
+// Dot products over the working nodes, or over the owned ones on a
+// partitioned mesh (each shared node counted once over the ranks).
 template <class V, int ND>
 void dots(sod_gpu_ctx *c, DotArgs<V, ND> A, double *out) {
-  k_dot<V, ND><<<DOT_BLOCKS, DOT_THREADS, 0, c->stream>>>(c->npoin_w, c->lpoin_w, A, c->cg.part, c->cg.dticket, out);
+  const bool part = c->halo.on;
+  k_dot<V, ND><<<DOT_BLOCKS, DOT_THREADS, 0, c->stream>>>(part ? c->halo.npoin_o : c->npoin_w,
+                                                          part ? c->halo.lpoin_o : c->lpoin_w, A, c->cg.part,
+                                                          c->cg.dticket, out);
 }
 
 int ensure_diag(sod_gpu_ctx *c) {
@@ -1761,8 +1779,18 @@ ImexCoef imex_coef(int S) {
 }
 
 // explicit convection (fact +1) of a stage state into a five-variable block
-void imex_convec(sod_gpu_ctx *c, const float *rho, const float *u, const float *q, const float *pr, const float *h,
-                 float *out) {
+// Halo sum of a five-variable block [mass][energy][mom x][mom y][mom z].
+int halo_block5(sod_gpu_ctx *c, float *out) {
+  HaloView v{};
+  const long long N = c->npoin;
+  v.width = 5;
+  v.nstride = 1;
+  for (int k = 0; k < 5; ++k) v.comp[k] = out + k * N;
+  return halo_sum(c, v);
+}
+
+int imex_convec(sod_gpu_ctx *c, const float *rho, const float *u, const float *q, const float *pr, const float *h,
+                float *out) {
   RhsArgs A{};
   A.rho = rho; A.u = u; A.q = q; A.pr = pr; A.E = h; A.fact_c = 1.0f;
   dispatch(c, [&](auto L) {
@@ -1771,10 +1799,11 @@ void imex_convec(sod_gpu_ctx *c, const float *rho, const float *u, const float *
   });
   const long long N = c->npoin;
   gather_res(c, out, out + 2 * N, out + N, 0, 0);
+  return halo_block5(c, out);
 }
 
 // diffusion without LPS (fact +1) into a five-variable block; rho_n null: rho
-void imex_diffusion(sod_gpu_ctx *c, const float *rho_n, const float *rho, const float *u, const float *Tem,
+int imex_diffusion(sod_gpu_ctx *c, const float *rho_n, const float *rho, const float *u, const float *Tem,
                     float *out) {
   auto &S = c->comp;
   RhsArgs A{};
@@ -1786,6 +1815,7 @@ void imex_diffusion(sod_gpu_ctx *c, const float *rho_n, const float *rho, const 
   });
   const long long N = c->npoin;
   gather_res(c, out, out + 2 * N, out + N, 0, 0);
+  return halo_block5(c, out);  // mod_solver_imex.f90:123, :196 (operator); time_integ_imex.f90:382 (stages)
 }
 
 // FP64 sum over the working nodes and the five variables of a (b - c)
@@ -1796,6 +1826,7 @@ double imex_dot(sod_gpu_ctx *c, const float *a, const float *b, const float *cc,
     A.a[k] = a + N * k; A.b[k] = b + N * k; A.c[k] = cc ? cc + N * k : nullptr;
   }
   dots<float, 5>(c, A, c->cg.dots + 8);
+  if ((*rc = allreduce(c, c->cg.dots + 8, 5, SOD_REDUCE_SUM_F64))) return 0.0;  // mod_solver_imex.f90:181, 225
   double t[5] = {0, 0, 0, 0, 0};
   if (cudaMemcpyAsync(t, c->cg.dots + 8, 40, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess) {
@@ -1821,11 +1852,12 @@ int imex_cg(sod_gpu_ctx *c, float fact, float dt, int maxIter, double tol) {
   CUDA_TRY(cudaMemcpyAsync(X.b + 2 * N, S.q32, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
   auto apply = [&](const float *v) {  // qn = v Ml + fact dt D(v)
     k_imex_prim<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, gm1, c->phys.Rgas, X.x, v, X.au, X.aT);
-    imex_diffusion(c, X.x, v, X.au, X.aT, X.qn);
+    int arc = imex_diffusion(c, X.x, v, X.au, X.aT, X.qn);
     k_imex_op<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, v, fact, dt, X.qn);
+    return arc;
   };
-  int rc = 0;
-  apply(X.x);
+  int rc = apply(X.x);
+  if (rc) return rc;
   k_imex_vec<<<nb, 256, 0, c->stream>>>(0, nw, N, c->lpoin_w, c->Ml, dt, 0.f, 0.f, X.b, X.x, X.r, X.p, X.qn, X.z,
                                         X.z1);
   const double auxB = std::sqrt(imex_dot(c, X.r, X.r, nullptr, &rc));
@@ -1833,7 +1865,7 @@ int imex_cg(sod_gpu_ctx *c, float fact, float dt, int maxIter, double tol) {
   double nrm = auxB;
   int it;
   for (it = 1; it <= maxIter; ++it) {
-    apply(X.p);
+    if ((rc = apply(X.p))) return rc;
     const double Q1 = imex_dot(c, X.r, X.z, nullptr, &rc);
     const double Q2 = imex_dot(c, X.p, X.qn, nullptr, &rc);
     if (rc) return rc;
@@ -1863,7 +1895,6 @@ extern "C" {
 int sod_gpu_comp_imex_step(sod_gpu_ctx *c, float dt, int maxIter, double tol) {
   if (!c || !c->comp.ready) return fail(SOD_GPU_EINVAL, "state not initialised");
   if (!(dt > 0.f) || maxIter < 1 || !(tol > 0.0)) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_comp_imex_step")) return prc;
   auto &S = c->comp;
   if (S.stages != 3 && S.stages != 4) return fail(SOD_GPU_EINVAL, "the IMEX integrator has 3 or 4 stages");
   if (S.fp64) return fail(SOD_GPU_EINVAL, "the IMEX integrator runs on the FP32 state (fp64_state = 0)");
@@ -1888,11 +1919,13 @@ int sod_gpu_comp_imex_step(sod_gpu_ctx *c, float dt, int maxIter, double tol) {
   if (S.first) {  // time_integ_imex.f90:240-273
     S.first = false;
     k_feta<<<nb, 256, 0, st>>>(nw, N, c->lpoin_w, S.u1, S.eta1, S.feta);
-    comp_entropy_pass(c, S.Reta1, false);
-    comp_visc(c, S.Reta1, S.rho32, S.u1, false);
     k_aux_h<<<nb, 256, 0, st>>>(nw, c->lpoin_w, gm / (gm - 1.0f), S.rho32, S.pr, X.aux_h);
-    imex_convec(c, S.rho32, S.u2, S.q32, S.pr, X.aux_h, X.R);
-    imex_diffusion(c, nullptr, S.rho32, S.u2, S.Tem, X.D);
+    if ((rc = comp_entropy_pass(c, S.Reta1, false)) || (rc = comp_visc(c, S.Reta1, S.rho32, S.u1, false)) ||
+        (rc = imex_convec(c, S.rho32, S.u2, S.q32, S.pr, X.aux_h, X.R)) ||
+        (rc = imex_diffusion(c, nullptr, S.rho32, S.u2, S.Tem, X.D))) {
+      c->async = was_async;
+      return rc;
+    }
   } else {  // the last stage's residuals open the step
     CUDA_TRY(cudaMemcpyAsync(X.R, X.R + (S.stages - 1) * B, B * 4, cudaMemcpyDeviceToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(X.D, X.D + (S.stages - 1) * B, B * 4, cudaMemcpyDeviceToDevice, st));
@@ -1906,13 +1939,22 @@ int sod_gpu_comp_imex_step(sod_gpu_ctx *c, float dt, int maxIter, double tol) {
     RhsArgs A{};
     A.rho = S.rho32; A.u = S.u2; A.Tem = S.Tem; A.mu_fluid = X.zmu; A.mue_t = X.zmue; A.musgs_t = nullptr;
     A.tau_stab = S.tau; A.proj12 = c->proj12; A.fact_d = 1.0f;
-    dispatch(c, [&](auto L) {
+    rc = dispatch(c, [&](auto L) {
       L.proj(c, true, S.rho32, S.u2, S.Tem);
       gather_proj_aos(c);
+      int hrc = halo_sum(c, halo_proj_view(c));
+      if (hrc) return hrc;
       L.template rhs<MODE_DIFF, IN_DIFF>(c, A);
       return 0;
     });
-    gather_res(c, X.stab, X.stab + 2 * N, X.stab + N, 0, 0);
+    if (!rc) {
+      gather_res(c, X.stab, X.stab + 2 * N, X.stab + N, 0, 0);
+      rc = halo_block5(c, X.stab);
+    }
+    if (rc) {
+      c->async = was_async;
+      return rc;
+    }
   }
   int iters = 0;
   for (int is = 2; is <= S.stages; ++is) {
@@ -1922,16 +1964,25 @@ int sod_gpu_comp_imex_step(sod_gpu_ctx *c, float dt, int maxIter, double tol) {
     k_eos_end<<<nb, 256, 0, st>>>(nw, N, c->lpoin_w, gm - 1.0f, gm, c->phys.Rgas, S.rho32, S.q32, S.E32, S.u2, S.eint,
                                   S.pr, S.csound, S.machno, S.Tem);
     k_aux_h<<<nb, 256, 0, st>>>(nw, c->lpoin_w, gm / (gm - 1.0f), S.rho32, S.pr, X.aux_h);
-    imex_convec(c, S.rho32, S.u2, S.q32, S.pr, X.aux_h, X.R + (is - 1) * B);
-    imex_diffusion(c, nullptr, S.rho32, S.u2, S.Tem, X.D + (is - 1) * B);
+    if ((rc = imex_convec(c, S.rho32, S.u2, S.q32, S.pr, X.aux_h, X.R + (is - 1) * B)) ||
+        (rc = imex_diffusion(c, nullptr, S.rho32, S.u2, S.Tem, X.D + (is - 1) * B))) {
+      c->async = was_async;
+      return rc;
+    }
   }
   X.cg_iters = iters;
   // entropy viscosity of the new state (time_integ_imex.f90:454-505)
   k_thermo_entropy<<<nb, 256, 0, st>>>(nw, N, c->lpoin_w, gm, c->phys.p_inf, c->phys.rho_inf, S.rho32, S.pr, S.u1,
                                        S.eta1, S.eta2, S.feta);
-  comp_entropy_pass(c, S.Reta2, true);
+  if ((rc = comp_entropy_pass(c, S.Reta2, true))) {
+    c->async = was_async;
+    return rc;
+  }
   k_aux_reta<<<nb, 256, 0, st>>>(nw, c->lpoin_w, dt, S.Reta1, S.Reta2, S.eta1, S.eta2, S.aux);
-  comp_visc(c, S.aux, S.rho32, S.u2, true);
+  if ((rc = comp_visc(c, S.aux, S.rho32, S.u2, true))) {
+    c->async = was_async;
+    return rc;
+  }
   k_sutherland<<<nb, 256, 0, st>>>(nw, c->lpoin_w, S.mu_factor, S.Tem, S.mu_fluid);
   c->async = was_async;
   return c->finish();
