@@ -33,9 +33,14 @@ def gpu():
 
 
 def _setup(gpu, porder, grid, Ma=0.5):
-    m = host.periodic_cube(porder, 4, jitter=0.05, seed=71, elem_shuffle=True, ordering=1)
+    if grid == "random":  # ragged parts on a non-cubic mesh
+        m = host.periodic_cube(porder, 3, 4, 5, jitter=0.05, seed=91, elem_shuffle=True, ordering=1)
+        pe = np.random.default_rng(92).integers(0, 3, m.nelem).astype(np.int32)
+    else:
+        m = host.periodic_cube(porder, 4, jitter=0.05, seed=71, elem_shuffle=True, ordering=1)
+        pe = partition.partition_elements(m, grid)
     ic = host.tgv_comp_init(m, Ma=Ma)
-    parts = partition.split(m, partition.partition_elements(m, grid))
+    parts = partition.split(m, pe)
     group = LocalHaloGroup([p.plan for p in parts], timeout=120.0)
     ctxs = []
     for p in parts:
@@ -45,7 +50,7 @@ def _setup(gpu, porder, grid, Ma=0.5):
     return m, ic, parts, group, ctxs
 
 
-@pytest.mark.parametrize("grid", [(1, 1, 2), (2, 1, 2), (2, 2, 2)])
+@pytest.mark.parametrize("grid", [(1, 1, 2), (2, 1, 2), (2, 2, 2), "random"])
 def test_halo_update_rank_ordered_sum(gpu, grid):
     m, ic, parts, group, ctxs = _setup(gpu, 3, grid)
     rng = np.random.default_rng(72)
@@ -70,7 +75,8 @@ def test_halo_update_rank_ordered_sum(gpu, grid):
         c.close()
 
 
-@pytest.mark.parametrize("porder,grid", [(3, (1, 1, 2)), (3, (2, 1, 2)), (4, (2, 1, 2)), (3, (2, 2, 2))])
+@pytest.mark.parametrize("porder,grid", [(3, (1, 1, 2)), (3, (2, 1, 2)), (4, (2, 1, 2)), (3, (2, 2, 2)),
+                                         (3, "random")])
 def test_partitioned_updateF_matches_whole_mesh(gpu, porder, grid):
     m, ic, parts, group, ctxs = _setup(gpu, porder, grid)
     rho, q, E = host.random_comp_state(m, seed=73)

@@ -63,6 +63,37 @@ def test_plan_invariants(grid):
         assert max(len(v) for v in owners.values()) == 8
 
 
+def test_ragged_random_partition_plan():
+    """A random element-to-part assignment on a non-cubic mesh (ragged parts,
+    nodes on all three ranks): every node's ranks list it, both sides of a
+    pair agree on the order, and each part's nodes are exactly the nodes
+    its elements touch."""
+    m = host.periodic_cube(3, 3, 4, 5, jitter=0.05, seed=91, elem_shuffle=True, ordering=1)
+    pe = np.random.default_rng(92).integers(0, 3, m.nelem).astype(np.int32)
+    parts = partition.split(m, pe)
+    n = m.nnode
+    cw = m.connecWork.reshape(n, m.nelem) - 1
+    owners = {}
+    for p in parts:
+        assert np.array_equal(p.nodes, np.unique(cw[:, p.elems]))
+        # local connectivity maps back to the global one
+        lc = p.mesh.connecWork.reshape(n, -1) - 1
+        assert np.array_equal(p.nodes[lc], cw[:, p.elems])
+        for g in p.nodes:
+            owners.setdefault(int(g), []).append(p.rank)
+    assert max(len(v) for v in owners.values()) == 3
+    for p in parts:
+        for nb in p.plan.ranksToComm.tolist():
+            a, b = p.plan.range_of(nb)
+            qa, qb = parts[nb].plan.range_of(p.rank)
+            assert np.array_equal(p.nodes[p.plan.nodesToComm[a:b] - 1],
+                                  parts[nb].nodes[parts[nb].plan.nodesToComm[qa:qb] - 1])
+    with pytest.raises(ValueError):
+        partition.split(m, np.zeros(m.nelem - 1, np.int32))
+    with pytest.raises(ValueError):
+        partition.split(m, np.full(m.nelem, 1, np.int32), nparts=2)  # part 0 empty
+
+
 def _rank_main(rank, world, port, grid, out_dir):
     import torch.distributed as dist
     from sod2d_b200.halo import DistHaloTransport
