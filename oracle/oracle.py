@@ -2,7 +2,8 @@
 
 ctypes binding of ``_build/liboracle.so``, the CPU restatement of the SOD2D
 reference arithmetic (``oracle_ops.hpp``).  Imported only by tests/,
-``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg, as the checker.
+``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg, as the reference
+arithmetic the CUDA results are compared with.
 """
 from __future__ import annotations
 

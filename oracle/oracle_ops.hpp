@@ -1,7 +1,8 @@
 // ORACLE -- test infrastructure only.  A CPU restatement of the SOD2D
 // reference's arithmetic for the spectral-element RHS hot path, used by
 // tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg as the
-// checker.  Never part of the product path.
+// arithmetic the CUDA results are compared with.  Never part of the
+// product path.
 //
 // Every routine follows the loop structure and operation order of the
 // Fortran routine it cites (paths relative to the reference project), in a
