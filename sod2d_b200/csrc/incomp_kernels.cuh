@@ -236,7 +236,28 @@ __global__ void __launch_bounds__(DOT_THREADS) k_dot(int npoin_w, const int *__r
   double s[ND];
 #pragma unroll
   for (int d = 0; d < ND; ++d) s[d] = 0.0;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npoin_w; t += gridDim.x * blockDim.x) {
+  // grid-stride over the nodes; four strides per trip with every load issued
+  // before the first product (same per-thread order as one stride per trip)
+  const int stride = gridDim.x * blockDim.x;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t + 3 * stride < npoin_w; t += 4 * stride) {
+    int p[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) p[u] = lpoin_w[t + u * stride];
+    V av[4][ND], bv[4][ND];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        av[u][d] = A.a[d][p[u]];
+        bv[u][d] = A.c[d] ? (V)(A.b[d][p[u]] - A.c[d][p[u]]) : A.b[d][p[u]];
+      }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) s[d] += (double)(av[u][d] * bv[u][d]);
+  }
+  for (; t < npoin_w; t += stride) {
     const int p = lpoin_w[t];
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
