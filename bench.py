@@ -585,6 +585,30 @@ def main():
     e2e_val = job_throughput(world, m.npoin_w, e2e_steps, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
     h2d = sum(t.numel() * 4 for t in h_in)
     d2h = sum(t.numel() * 4 for t in h_out[0])
+
+    # the copies alone, same buffers and streams, both directions at once:
+    # the bound the end-to-end number can reach over the host link
+    def copies_only(nsteps):
+        for k in range(nsteps):
+            b = k % 2
+            with torch.cuda.stream(s_up):
+                for hd, dd in zip(h_in, d_in[b]):
+                    dd.copy_(hd, non_blocking=True)
+            with torch.cuda.stream(s_dn):
+                for ho, dd in zip(h_out[b], d_out[b]):
+                    ho.copy_(dd, non_blocking=True)
+
+    copies_only(2)
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(s_up)
+    s_dn.wait_event(c0)
+    copies_only(e2e_steps)
+    s_dn.wait_stream(s_up)
+    c1.record(s_dn)
+    c1.synchronize()
+    copy_ms = max_over_ranks(c0.elapsed_time(c1), world, "cuda")
+    copy_bound = job_throughput(world, m.npoin_w, e2e_steps, copy_ms)
     # the pipelined result must equal the device-resident one
     torch.cuda.synchronize()
     e2e_check = max(float((h_out[(e2e_steps - 1) % 2][i].cuda() - out[i]).abs().max()) for i in range(3))
@@ -605,7 +629,10 @@ def main():
         "e2e": {"value": round(e2e_val, 2), "unit": "Mnode-stages/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                 "pipelining": "H2D(k+1) and D2H(k-1) overlap RHS(k) on 3 streams, double buffers",
-                "max_abs_diff_vs_device_resident": e2e_check},
+                "max_abs_diff_vs_device_resident": e2e_check,
+                "copy_bound": {"value": round(copy_bound, 2), "frac": round(e2e_val / copy_bound, 4),
+                               "link_gbs_per_direction": round(max(h2d, d2h) * e2e_steps / (copy_ms / 1e3) / 1e9, 1),
+                               "what": "the same H2D and D2H copies alone, both directions at once"}},
         "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
         "device_bytes": ctx.device_bytes,
