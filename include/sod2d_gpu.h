@@ -139,10 +139,16 @@ int sod_gpu_halo_update(sod_gpu_ctx *ctx, float *field, int ncomp);
  * reductions of rk_4_ls_main and imex_main; the IMEX solve's dot products
  * run over the working nodes this rank owns (a shared node belongs to the
  * lowest rank holding it; the reference's lpoin_o) and are summed over the
- * ranks.  The incompressible entry points whose solves need global dot
- * products (sod_gpu_conjgrad_pressure, sod_gpu_pressure_solve,
- * sod_gpu_conjgrad_veloc, sod_gpu_incomp_*) return SOD_GPU_EINVAL on a
- * context with a halo plan. */
+ * ranks.  The incompressible operators (Laplacian, its diagonal, gradient,
+ * divergence, velocity projection) sum over the ranks inside, as the
+ * reference's mod_operators.f90 does; sod_gpu_conjgrad_pressure and
+ * sod_gpu_conjgrad_veloc sum their operators and reduce their dot products
+ * over the owned nodes; sod_gpu_incomp_step (with precond 2, the reference's
+ * FP32 pressure solve), sod_gpu_incomp_adapt_dt and sod_gpu_incomp_analysis
+ * run a partitioned mesh.  The FP64-certified solve
+ * (sod_gpu_pressure_solve, sod_gpu_incomp_step with precond 0 or 1) and
+ * sod_gpu_eval_laplacian_mult64 return SOD_GPU_EINVAL on a context with a
+ * halo plan. */
 #define SOD_REDUCE_MIN_F32 0
 #define SOD_REDUCE_MAX_F32 1
 #define SOD_REDUCE_SUM_F64 2

@@ -354,6 +354,15 @@ HaloView halo_res_view(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener) 
   return v;
 }
 
+// View of ncomp reference-layout components (npoin each) of one array.
+HaloView halo_soa_view(sod_gpu_ctx *c, float *a, int ncomp) {
+  HaloView v{};
+  v.width = ncomp;
+  v.nstride = 1;
+  for (int k = 0; k < ncomp; ++k) v.comp[k] = a + (long long)k * c->npoin;
+  return v;
+}
+
 // In-place global reduction of a device buffer (no-op without a callback).
 int allreduce(sod_gpu_ctx *c, void *buf, int count, int kind) {
   auto &h = c->halo;
@@ -603,6 +612,7 @@ int sod_gpu_set_halo(sod_gpu_ctx *c, int rank, int nnb, const int *ranksToComm, 
     h.own.clear();
     return rc;
   }
+  c->cg.have_diag = false;  // the Jacobi diagonal is assembled over the ranks from now on
   h.rank = rank;
   h.nsend = (int)nsend;
   h.nuniq = (int)uniq.size();
@@ -883,6 +893,7 @@ int ensure_diag(sod_gpu_ctx *c) {
     return 0;
   });
   k_gather1<float><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, G.diag, 0);
+  if ((rc = halo_sum(c, halo_soa_view(c, G.diag, 1)))) return rc;  // mod_operators.f90:677
   G.have_diag = true;
   return 0;
 }
@@ -980,11 +991,13 @@ int sod_gpu_eval_laplacian_mult(sod_gpu_ctx *c, const float *p, float *ResP) {
   if (!c || !p || !ResP) return fail(SOD_GPU_EINVAL, "bad argument");
   CUDA_TRY(cudaMemsetAsync(ResP, 0, (size_t)c->npoin * 4, c->stream));
   lap<float>(c, p, ResP);
-  return c->finish();
+  int rc = halo_sum(c, halo_soa_view(c, ResP, 1));  // mod_operators.f90:102
+  return rc ? rc : c->finish();
 }
 
 int sod_gpu_eval_laplacian_mult64(sod_gpu_ctx *c, const double *p, double *ResP) {
   if (!c || !p || !ResP) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (int prc = no_partition(c, "sod_gpu_eval_laplacian_mult64")) return prc;
   CUDA_TRY(cudaMemsetAsync(ResP, 0, (size_t)c->npoin * 8, c->stream));
   lap<double>(c, p, ResP);
   return c->finish();
@@ -1009,7 +1022,8 @@ int sod_gpu_eval_gradient(sod_gpu_ctx *c, const float *x, float *gradX) {
   const long long N = c->npoin;
   o.p[0] = gradX; o.p[1] = gradX + N; o.p[2] = gradX + 2 * N;
   k_gather<4, 3, false><<<nblk(N, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, nullptr, o, 0, 1);
-  return c->finish();
+  int rc = halo_sum(c, halo_soa_view(c, gradX, 3));  // mod_operators.f90:274
+  return rc ? rc : c->finish();
 }
 
 int sod_gpu_eval_divergence(sod_gpu_ctx *c, const float *u, float *divU) {
@@ -1022,7 +1036,8 @@ int sod_gpu_eval_divergence(sod_gpu_ctx *c, const float *u, float *divU) {
   OutPtrs o{};
   o.p[0] = divU;
   k_gather<4, 1, false><<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, nullptr, o, 0, 0);
-  return c->finish();
+  int rc = halo_sum(c, halo_soa_view(c, divU, 1));  // mod_operators.f90:566
+  return rc ? rc : c->finish();
 }
 
 int sod_gpu_full_convec_ijk_incomp(sod_gpu_ctx *c, const float *u, const float *q, float *Rmom) {
@@ -1042,7 +1057,6 @@ int sod_gpu_full_convec_ijk_incomp(sod_gpu_ctx *c, const float *u, const float *
 int sod_gpu_conjgrad_pressure(sod_gpu_ctx *c, const float *Rp0, float *R, int maxIter, double tol, int *iters,
                               double *res_rel) {
   if (!c || !Rp0 || !R || maxIter < 1) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_conjgrad_pressure")) return prc;
   int rc;
   if ((rc = ensure_diag(c)) || (rc = ensure_cg32(c))) return rc;
   auto &G = c->cg;
@@ -1051,6 +1065,7 @@ int sod_gpu_conjgrad_pressure(sod_gpu_ctx *c, const float *Rp0, float *R, int ma
   for (float *z : {G.x32, G.r32, G.p32, G.q32, G.z032, G.z132, G.b32}) CUDA_TRY(cudaMemsetAsync(z, 0, N * 4, st));
   // b = R - A x0 ; r0 = b ; z0 = r0 / M ; p0 = z0   (mod_solver_incomp.f90:310-350)
   lap<float>(c, Rp0, G.q32);
+  if ((rc = halo_sum(c, halo_soa_view(c, G.q32, 1)))) return rc;
   const int nw = c->npoin_w;
   k_axpby<float><<<nblk(nw, 256), 256, 0, st>>>(nw, c->lpoin_w, -1.f, G.q32, 0.f, G.b32);
   k_axpby<float><<<nblk(nw, 256), 256, 0, st>>>(nw, c->lpoin_w, 1.f, R, 1.f, G.b32);
@@ -1059,6 +1074,7 @@ int sod_gpu_conjgrad_pressure(sod_gpu_ctx *c, const float *Rp0, float *R, int ma
     // z0 = r0 / M, p0 = z0 via one update with a = 0
     DotArgs<float, 1> A{{G.b32}, {G.b32}, {nullptr}};
     dots<float, 1>(c, A, G.dots + 6);  // ||b||^2
+    if ((rc = allreduce(c, G.dots + 6, 1, SOD_REDUCE_SUM_F64))) return rc;  // mod_solver_incomp.f90:366
   }
   // z0 = r/M
   {
@@ -1076,11 +1092,14 @@ int sod_gpu_conjgrad_pressure(sod_gpu_ctx *c, const float *Rp0, float *R, int ma
   double nrm = auxB;
   for (it = 1; it <= maxIter; ++it) {
     lap<float>(c, G.p32, G.q32);
+    if ((rc = halo_sum(c, halo_soa_view(c, G.q32, 1)))) return rc;
     dots<float, 2>(c, DotArgs<float, 2>{{G.r32, G.p32}, {G.z032, G.q32}, {nullptr, nullptr}}, G.dots);  // Q1, Q2
+    if ((rc = allreduce(c, G.dots, 2, SOD_REDUCE_SUM_F64))) return rc;  // mod_solver_incomp.f90:388
     k_cg_update1<float><<<nblk(nw, 256), 256, 0, st>>>(nw, c->lpoin_w, G.dots, G.x32, G.r32, G.p32, G.q32, G.z032,
                                                        G.z132, G.diag, 1, 1);
     // ||r||^2 and <r, z0 - z1>
     dots<float, 2>(c, DotArgs<float, 2>{{G.r32, G.r32}, {G.r32, G.z032}, {nullptr, G.z132}}, G.dots + 2);
+    if ((rc = allreduce(c, G.dots + 2, 2, SOD_REDUCE_SUM_F64))) return rc;  // mod_solver_incomp.f90:415, 437
     double h[2];
     CUDA_TRY(cudaMemcpyAsync(h, G.dots + 2, 16, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
@@ -2567,13 +2586,19 @@ int ensure_velo(sod_gpu_ctx *c) {
 }
 
 // LPS projection of v into V.tauP (node-major, mass-divided)
-void velo_tau(sod_gpu_ctx *c, const float *v) {
+int velo_tau(sod_gpu_ctx *c, const float *v) {
   dispatch(c, [&](auto L) {
     using LL = decltype(L);
     k_tauv_elem<LL::P_, LL::EPB><<<LL::grid(c->nelem), LL::TPB, 0, c->stream>>>(c->md(), v, c->slotsB);
     return 0;
   });
   k_gather_tauv<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, c->Ml, c->velo.tauP);
+  // halo sum of the six projected components (mod_operators.f90:467-469)
+  HaloView hv{};
+  hv.width = 6;
+  hv.nstride = 8;
+  for (int k = 0; k < 6; ++k) hv.comp[k] = c->velo.tauP + k;
+  return halo_sum(c, hv);
 }
 
 // out (npoin,3) = full_diff_stab_incomp(v) with the projection in V.tauP
@@ -2601,6 +2626,8 @@ int velo_dots(sod_gpu_ctx *c, const float *a0, const float *b0, const float *c0,
     A.a[3 + d] = a1 ? a1 + N * d : a0 + N * d; A.b[3 + d] = b1 ? b1 + N * d : b0 + N * d; A.c[3 + d] = nullptr;
   }
   dots<float, 6>(c, A, c->cg.dots + 8);
+  int rc = allreduce(c, c->cg.dots + 8, 6, SOD_REDUCE_SUM_F64);  // mod_solver_incomp.f90:128-229
+  if (rc) return rc;
   double t[6];
   CUDA_TRY(cudaMemcpyAsync(t, c->cg.dots + 8, 48, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -2625,7 +2652,7 @@ int sod_gpu_eval_tau_veloc(sod_gpu_ctx *c, const float *u, float *GradX, float *
   if (!c || !u || !GradX || !GradY || !GradZ) return fail(SOD_GPU_EINVAL, "bad argument");
   int rc;
   if ((rc = ensure_velo(c))) return rc;
-  velo_tau(c, u);
+  if ((rc = velo_tau(c, u))) return rc;
   k_unpack_tauv<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, c->velo.tauP, GradX, GradY, GradZ);
   return c->finish();
 }
@@ -2650,7 +2677,6 @@ int sod_gpu_full_diff_stab_incomp(sod_gpu_ctx *c, const float *u, const float *m
 int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu_fluid, const float *mu_sgs,
                            const float *Rp0, float *R, int maxIter, double tol, int *iters, double *res_rel) {
   if (!c || !mu_fluid || !Rp0 || !R || maxIter < 1 || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_conjgrad_veloc")) return prc;
   if (!c->helem) return fail(SOD_GPU_EINVAL, "conjgrad_veloc needs helem at init");
   int rc;
   if ((rc = ensure_velo(c))) return rc;
@@ -2671,11 +2697,15 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu
   k_species_tau<<<nblk(c->nelem, 8), 256, 0, c->stream>>>(c->nelem, c->N, c->conn, c->helem, V.x, N,
                                                           c->phys.c_species_stab / (float)c->P, V.tau_e);
   auto apply = [&](const float *v) {  // q = v Ml + fact dt D(v)
-    velo_tau(c, v);
+    int arc = velo_tau(c, v);
+    if (arc) return arc;
     velo_diff(c, v, mu_fluid, musgs, V.tau_e, V.q);
+    // halo sum of the operator (mod_solver_incomp.f90:94, :146)
+    if ((arc = halo_sum(c, halo_soa_view(c, V.q, 3)))) return arc;
     k_veloc_op<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, v, fact, dt, V.q);
+    return 0;
   };
-  apply(V.x);
+  if ((rc = apply(V.x))) { c->async = was_async; return rc; }
   k_veloc_vec<<<nb, 256, 0, c->stream>>>(0, nw, N, c->lpoin_w, c->Ml, dt, 0.f, 0.f, V.b, V.x, V.r, V.p, V.q, V.z,
                                          V.z1);
   double h[2];
@@ -2684,7 +2714,7 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu
   double nrm = auxB;
   int it;
   for (it = 1; it <= maxIter; ++it) {
-    apply(V.p);
+    if ((rc = apply(V.p))) { c->async = was_async; return rc; }
     if ((rc = velo_dots(c, V.r, V.z, nullptr, V.p, V.q, h))) { c->async = was_async; return rc; }
     const double Q1 = h[0];
     const float alpha = (float)(h[0] / h[1]);
@@ -2709,7 +2739,6 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu
 
 int sod_gpu_incomp_init(sod_gpu_ctx *c, const float *u, double nu) {
   if (!c || !u || nu < 0) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_incomp_init")) return prc;
   if (!c->helem) return fail(SOD_GPU_EINVAL, "the incompressible step needs helem at init");
   auto &I = c->inc;
   const size_t N = c->npoin;
@@ -2761,7 +2790,9 @@ int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *c, int *iters, double *res_rel) {
 
 int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats) {
   if (!c || !c->inc.ready || !opts || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_incomp_step")) return prc;
+  // a partitioned mesh runs the reference's FP32 pressure solve (precond 2)
+  if (opts->precond != 2)
+    if (int prc = no_partition(c, "sod_gpu_incomp_step with the FP64-certified solve")) return prc;
   auto &I = c->inc;
   const long long N = c->npoin;
   const int nw = c->npoin_w;
@@ -2772,6 +2803,7 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
   c->async = true;  // chain the operator calls; synchronise at the end
   // Rmom(:,:,2) = full_convec_ijk_incomp(u1, u1 rho, rho), rho = 1
   int rc = sod_gpu_full_convec_ijk_incomp(c, u1, u1, I.Rm[1]);
+  if (!rc) rc = halo_sum(c, halo_soa_view(c, I.Rm[1], 3));  // time_integ_incomp.f90:315
   if (rc) { c->async = was_async; return rc; }
   k_bdf_ext<<<nb, 256, 0, c->stream>>>(nw, N, c->lpoin_w, c->Ml, I.Rm[1], I.Rm[0], I.Rm[2], u1, u3, u4, k, dt, u2);
   {  // Rmom(:,:,3) = Rmom(:,:,1); Rmom(:,:,1) = Rmom(:,:,2)
@@ -2854,7 +2886,6 @@ int sod_gpu_incomp_set_pressure(sod_gpu_ctx *c, const double *p) {
 
 int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float *dt) {
   if (!c || !c->inc.ready || !dt || !(cfl_conv > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_incomp_adapt_dt")) return prc;
   auto &I = c->inc;
   const unsigned init_bits = 0x56B5E621u;  // 1e14f, the reference's initial dt_conv
   CUDA_TRY(cudaMemcpyAsync(I.bits, &init_bits, 4, cudaMemcpyHostToDevice, c->stream));
@@ -2865,6 +2896,7 @@ int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float *dt) {
                                                             I.one, cfl_conv, 1.0f, I.bits);
     return 0;
   });
+  if (int rrc = allreduce(c, I.bits, 1, SOD_REDUCE_MIN_F32)) return rrc;  // mod_time_ops.f90:212
   unsigned b = 0;
   CUDA_TRY(cudaMemcpyAsync(&b, I.bits, 4, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -2874,7 +2906,6 @@ int sod_gpu_incomp_adapt_dt(sod_gpu_ctx *c, float cfl_conv, float *dt) {
 
 int sod_gpu_incomp_analysis(sod_gpu_ctx *c, double *out) {
   if (!c || !c->inc.ready || !out) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_incomp_analysis")) return prc;
   auto &I = c->inc;
   dispatch(c, [&](auto L) {
     using LL = decltype(L);
@@ -2883,6 +2914,7 @@ int sod_gpu_incomp_analysis(sod_gpu_ctx *c, double *out) {
     return 0;
   });
   k_sum_parts<<<1, 1024, 0, c->stream>>>(c->nelem, I.part, I.sums);
+  if (int rrc = allreduce(c, I.sums, 3, SOD_REDUCE_SUM_F64)) return rrc;  // mod_analysis.f90:39, 134-135
   double sums[3];
   CUDA_TRY(cudaMemcpyAsync(sums, I.sums, 24, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));

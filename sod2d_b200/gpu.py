@@ -354,11 +354,20 @@ class IncompSolver:
     SolveOpts for the pressure solve (precond 2: the reference's FP32 CG);
     veloc = (maxIter, tol) of the velocity solve."""
 
-    def __init__(self, mesh, Re=1600.0, cfl_conv=0.5, veloc=(20, 1e-2)):
+    def __init__(self, mesh, Re=1600.0, cfl_conv=0.5, veloc=(20, 1e-2), partition=None):
+        """partition = (part, transport): run the rank `part` of `mesh` with
+        its halo sums and global reductions (a collective constructor; the
+        steps must use the reference's FP32 pressure solve, precond 2)."""
         import torch
         self.torch = torch
+        if partition is not None:
+            part, transport = partition
+            mesh = part.mesh
         self.mesh = mesh
         self.ctx = Context(mesh, default_phys())
+        if partition is not None:
+            self.ctx.set_halo(part.plan, transport)
+            self.ctx.set_allreduce(transport, part.rank)
         N = mesh.npoin
         x, y, z = (mesh.coord[i * N:(i + 1) * N].astype(np.float32) for i in range(3))
         u0 = np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z),

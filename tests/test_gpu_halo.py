@@ -280,20 +280,72 @@ def test_partitioned_imex_loop_matches_whole_mesh(gpu, porder, grid, stages):
     assert rel.max() < 1e-4
 
 
+@pytest.mark.parametrize("porder,grid", [(3, (2, 1, 2)), (4, (2, 2, 2))])
+def test_partitioned_incomp_loop_matches_whole_mesh(gpu, porder, grid):
+    """bdfext3_main_incomp on a partitioned mesh with the reference's FP32
+    solves (conjGrad_pressure_incomp and conjGrad_veloc_incomp at maxIter 20,
+    tol 1e-2): halo sums inside the Laplacian, its diagonal, the gradient,
+    the divergence and the velocity projection, on the convection and on the
+    velocity operator; CG dots over owned nodes summed over the ranks; the
+    dt and analysis reductions.  The parts agree bit for bit; the pressure
+    and velocity CG iterations equal the whole-mesh run's and the analysis
+    rows match it."""
+    m = host.periodic_cube(porder, 4, jitter=0.05, seed=79, elem_shuffle=True, ordering=1)
+    opts = gpu.SolveOpts(20, 1e-2, 2, 50, 0)
+    nsteps = 8
+
+    def run(s):
+        rows, its = [s.analysis()], []
+        for _ in range(nsteps):
+            s.step(opts)
+            vi, vr = C.c_int(), C.c_double()
+            s.ctx.call("sod_gpu_incomp_veloc_stats", C.byref(vi), C.byref(vr))
+            its.append((s.stats.iterations, vi.value))
+            rows.append(s.analysis())
+            s.dt = s.adapt_dt()
+        return np.array(rows), its
+
+    whole = gpu.IncompSolver(m, Re=1600.0, cfl_conv=0.5, veloc=(20, 1e-2))
+    hw, itw = run(whole)
+    whole.close()
+    parts = partition.split(m, partition.partition_elements(m, grid))
+    group = LocalHaloGroup([p.plan for p in parts], timeout=120.0)
+    solvers = group.run([lambda p=p: gpu.IncompSolver(m, Re=1600.0, cfl_conv=0.5, veloc=(20, 1e-2),
+                                                      partition=(p, group)) for p in parts])
+    out = group.run([lambda s=s: run(s) for s in solvers])
+    for s in solvers:
+        s.close()
+    for h, its in out[1:]:
+        assert np.array_equal(h, out[0][0]) and its == out[0][1]
+    hp, itp = out[0]
+    print(f"P={porder} {len(parts)} parts: (pressure, velocity) CG iterations whole {itw} parts {itp}")
+    assert itp == itw
+    rel = np.abs(hp[:, :5] - hw[:, :5]) / np.maximum(np.abs(hw[:, :5]), 1e-30)
+    print("max relative difference per column (time, EK, eps_S, eps_D, eps_T)", rel.max(axis=0))
+    assert rel.max() < 1e-4
+
+
 def test_partition_refuses_global_solves(gpu):
-    """Entry points whose solves take global dot products refuse a context
-    with a halo plan instead of returning a rank-local answer."""
+    """The entry points whose solves need global dot products inside a
+    device-resident iteration (the FP64-certified pressure solve and the
+    incompressible step that uses it) refuse a context with a halo plan
+    instead of returning a rank-local answer."""
     m = host.periodic_cube(3, 4, seed=77)
     parts = partition.split(m, partition.partition_elements(m, (1, 1, 2)))
     p = parts[0]
     ctx = gpu.Context(p.mesh, gpu.default_phys())
     group = LocalHaloGroup([p.plan], timeout=10.0)  # never exchanges here
     ctx.set_halo(p.plan, group)
-    x = torch.zeros(p.mesh.npoin, device="cuda")
-    it, res = C.c_int(), C.c_double()
+    N = p.mesh.npoin
+    b, x = torch.zeros(N, dtype=torch.float64, device="cuda"), torch.zeros(N, dtype=torch.float64, device="cuda")
+    st = gpu.SolveStats()
     with pytest.raises(RuntimeError, match="halo plan"):
-        ctx.call("sod_gpu_conjgrad_pressure", gpu.dptr(x), gpu.dptr(x), 10, 1e-8, C.byref(it), C.byref(res))
-    u = torch.zeros(3 * p.mesh.npoin, device="cuda")
+        ctx.call("sod_gpu_pressure_solve", gpu.dptr(b), gpu.dptr(x), C.byref(gpu.SolveOpts(10, 1e-8, 0, 50, 0)),
+                 C.byref(st))
     with pytest.raises(RuntimeError, match="halo plan"):
-        ctx.call("sod_gpu_incomp_init", gpu.dptr(u), 1e-3)
+        ctx.call("sod_gpu_eval_laplacian_mult64", gpu.dptr(b), gpu.dptr(x))
+    u = torch.zeros(3 * N, device="cuda")
+    ctx.call("sod_gpu_incomp_init", gpu.dptr(u), 1e-3)
+    with pytest.raises(RuntimeError, match="halo plan"):
+        ctx.call("sod_gpu_incomp_step", C.c_float(1e-3), C.byref(gpu.SolveOpts(10, 1e-8, 0, 50, 0)), C.byref(st))
     ctx.close()
