@@ -145,10 +145,12 @@ int sod_gpu_halo_update(sod_gpu_ctx *ctx, float *field, int ncomp);
  * sod_gpu_conjgrad_veloc sum their operators and reduce their dot products
  * over the owned nodes; sod_gpu_incomp_step (with precond 2, the reference's
  * FP32 pressure solve), sod_gpu_incomp_adapt_dt and sod_gpu_incomp_analysis
- * run a partitioned mesh.  The FP64-certified solve
- * (sod_gpu_pressure_solve, sod_gpu_incomp_step with precond 0 or 1) and
- * sod_gpu_eval_laplacian_mult64 return SOD_GPU_EINVAL on a context with a
- * halo plan. */
+ * run a partitioned mesh.  sod_gpu_pressure_solve with precond 0 runs a
+ * host-driven FP64 Jacobi-PCG on a partitioned mesh (FP64 values travel as
+ * two floats each through the exchange, so send_buf and recv_buf must be
+ * 8-byte aligned), certified on the true residual like the single-rank
+ * solve; the learned preconditioner (precond 1), whose patches cross the
+ * part boundaries, returns SOD_GPU_EINVAL on a context with a halo plan. */
 #define SOD_REDUCE_MIN_F32 0
 #define SOD_REDUCE_MAX_F32 1
 #define SOD_REDUCE_SUM_F64 2

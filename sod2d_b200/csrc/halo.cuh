@@ -25,18 +25,22 @@ constexpr int HALO_MAX_WIDTH = 12;
 
 // Component k of node p is comp[k][p * nstride]: a node-major buffer of
 // width W (comp[k] = base + k, nstride = W) or reference-layout (npoin,ncomp)
-// arrays (comp[k] = base + k*npoin, nstride = 1).
-struct HaloView {
-  float *comp[HALO_MAX_WIDTH];
+// arrays (comp[k] = base + k*npoin, nstride = 1).  T is float, or double for
+// the FP64 pressure solve (a double travels as two floats of the buffers).
+template <class T>
+struct HaloViewT {
+  T *comp[HALO_MAX_WIDTH];
   int width;
   long long nstride;
 };
+using HaloView = HaloViewT<float>;
 
-__global__ void k_halo_pack(int nsend, const int *__restrict__ node, HaloView v, float *__restrict__ buf) {
+template <class T>
+__global__ void k_halo_pack(int nsend, const int *__restrict__ node, HaloViewT<T> v, T *__restrict__ buf) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nsend) return;
   const long long p = (long long)node[j] * v.nstride;
-  float val[HALO_MAX_WIDTH];
+  T val[HALO_MAX_WIDTH];
 #pragma unroll
   for (int k = 0; k < HALO_MAX_WIDTH; ++k)
     if (k < v.width) val[k] = v.comp[k][p];
@@ -47,18 +51,19 @@ __global__ void k_halo_pack(int nsend, const int *__restrict__ node, HaloView v,
 
 // For shared node u: contributions ptr[u]..ptr[u+1]-1 in ascending rank
 // order; src < 0 is this rank's own value, else a position in recv.
+template <class T>
 __global__ void k_halo_sum(int nuniq, const int *__restrict__ uniq_node, const int *__restrict__ ptr,
-                           const int *__restrict__ src, HaloView v, const float *__restrict__ recv) {
+                           const int *__restrict__ src, HaloViewT<T> v, const T *__restrict__ recv) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nuniq) return;
   const long long p = (long long)uniq_node[u] * v.nstride;
   const int b = ptr[u], e = ptr[u + 1];
   for (int k = 0; k < v.width; ++k) {
-    const float own = v.comp[k][p];
-    float acc = 0.f;
+    const T own = v.comp[k][p];
+    T acc = 0;
     for (int i = b; i < e; ++i) {
       const int s = src[i];
-      const float x = s < 0 ? own : recv[(long long)s * v.width + k];
+      const T x = s < 0 ? own : recv[(long long)s * v.width + k];
       acc = i == b ? x : acc + x;
     }
     v.comp[k][p] = acc;

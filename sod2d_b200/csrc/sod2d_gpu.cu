@@ -323,16 +323,22 @@ void gather_proj_aos(sod_gpu_ctx *c) {
 
 // Sum the view's components over the ranks that share each node (no-op
 // without a halo plan).
-int halo_sum(sod_gpu_ctx *c, const HaloView &v) {
+template <class T>
+int halo_sum(sod_gpu_ctx *c, const HaloViewT<T> &v) {
   auto &h = c->halo;
   if (!h.on) return 0;
+  static_assert(sizeof(T) % sizeof(float) == 0, "values travel as whole floats");
+  if ((int)(v.width * sizeof(T) / sizeof(float)) > HALO_MAX_WIDTH)
+    return fail(SOD_GPU_EINVAL, "halo exchange wider than the buffers");
   if (h.nsend > 0)
-    k_halo_pack<<<nblk(h.nsend, 256), 256, 0, c->stream>>>(h.nsend, h.send_node, v, h.send);
+    k_halo_pack<T><<<nblk(h.nsend, 256), 256, 0, c->stream>>>(h.nsend, h.send_node, v, (T *)h.send);
   CUDA_TRY(cudaGetLastError());
-  if (h.fn(h.user, h.send, h.recv, v.width, (void *)c->stream) != 0)
+  const int width_floats = v.width * (int)(sizeof(T) / sizeof(float));
+  if (h.fn(h.user, h.send, h.recv, width_floats, (void *)c->stream) != 0)
     return fail(SOD_GPU_EINVAL, "halo exchange callback failed");
   if (h.nuniq > 0)
-    k_halo_sum<<<nblk(h.nuniq, 128), 128, 0, c->stream>>>(h.nuniq, h.uniq_node, h.ptr, h.src, v, h.recv);
+    k_halo_sum<T><<<nblk(h.nuniq, 128), 128, 0, c->stream>>>(h.nuniq, h.uniq_node, h.ptr, h.src, v,
+                                                             (const T *)h.recv);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -997,10 +1003,14 @@ int sod_gpu_eval_laplacian_mult(sod_gpu_ctx *c, const float *p, float *ResP) {
 
 int sod_gpu_eval_laplacian_mult64(sod_gpu_ctx *c, const double *p, double *ResP) {
   if (!c || !p || !ResP) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_eval_laplacian_mult64")) return prc;
   CUDA_TRY(cudaMemsetAsync(ResP, 0, (size_t)c->npoin * 8, c->stream));
   lap<double>(c, p, ResP);
-  return c->finish();
+  HaloViewT<double> hv{};
+  hv.width = 1;
+  hv.nstride = 1;
+  hv.comp[0] = ResP;
+  int rc = halo_sum<double>(c, hv);  // mod_operators.f90:102
+  return rc ? rc : c->finish();
 }
 
 int sod_gpu_eval_laplacian_diag(sod_gpu_ctx *c, float *d) {
@@ -1167,6 +1177,124 @@ __global__ void k_resid(int npoin_w, const int *__restrict__ lpoin_w, const doub
   r[i] = b[i] - q[i];
 }
 
+// b -= sc[0] / sc[1] on the working nodes (sum and count of the mean)
+__global__ void k_sub_ratio(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ sc,
+                            double *__restrict__ b) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  b[lpoin_w[t]] -= sc[0] / sc[1];
+}
+
+// z = M r on the working nodes
+__global__ void k_mul_w(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ M,
+                        const double *__restrict__ r, double *__restrict__ z) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npoin_w) return;
+  const int i = lpoin_w[t];
+  z[i] = M[i] * r[i];
+}
+
+// The FP64 Jacobi-PCG of sod_gpu_pressure_solve on a partitioned mesh,
+// driven from the host: the Laplacian and its diagonal are summed over the
+// ranks, the mean of b and every dot product run over the owned nodes and
+// are summed over the ranks (the reference's lpoin_o and MPI_Allreduce,
+// mod_solver_incomp.f90:366-437), and convergence is declared on the true
+// FP64 residual ||b - A x|| / ||b||, as in the single-rank solve.
+int pressure_solve_parts(sod_gpu_ctx *c, const double *b_in, double *x, const sod_solve_opts_t *opts,
+                         sod_solve_stats_t *stats) {
+  int rc;
+  if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c))) return rc;
+  auto &G = c->cg;
+  auto &h = c->halo;
+  const size_t N = c->npoin;
+  const int nw = c->npoin_w;
+  const cudaStream_t st = c->stream;
+  const unsigned nb = nblk(nw, 256);
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  CUDA_TRY(cudaEventRecord(e0, st));
+  k_inv_diag64<<<nblk(N, 256), 256, 0, st>>>((long long)N, G.diag, G.Minv);
+  CUDA_TRY(cudaMemcpyAsync(G.b, b_in, N * 8, cudaMemcpyDeviceToDevice, st));
+  // mean of b over the whole mesh: sum and count over the owned nodes
+  k_sum_partial<<<DOT_BLOCKS, DOT_THREADS, 0, st>>>(h.npoin_o, h.lpoin_o, G.b, G.part);
+  k_dot_final<<<1, 1024, 0, st>>>(1, G.part, G.dots + 7);
+  const double cnt = (double)h.npoin_o;
+  CUDA_TRY(cudaMemcpyAsync(G.dots + 8, &cnt, 8, cudaMemcpyHostToDevice, st));
+  if ((rc = allreduce(c, G.dots + 7, 2, SOD_REDUCE_SUM_F64))) return rc;
+  k_sub_ratio<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.dots + 7, G.b);
+  auto apply = [&](const double *v, double *out) -> int {
+    lap<double>(c, v, out);
+    HaloViewT<double> hv{};
+    hv.width = 1;
+    hv.nstride = 1;
+    hv.comp[0] = out;
+    return halo_sum<double>(c, hv);
+  };
+  // a . b and c . d over the owned nodes, summed over the ranks
+  auto dot2 = [&](const double *a, const double *bb, const double *cc, const double *dd, double *out2) -> int {
+    dots<double, 2>(c, DotArgs<double, 2>{{a, cc}, {bb, dd}, {nullptr, nullptr}}, G.dots);
+    int r2 = allreduce(c, G.dots, 2, SOD_REDUCE_SUM_F64);
+    if (r2) return r2;
+    CUDA_TRY(cudaMemcpyAsync(out2, G.dots, 16, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
+  };
+  double d2[2];
+  if ((rc = dot2(G.b, G.b, G.b, G.b, d2))) return rc;
+  const double bnorm = std::sqrt(d2[0]);
+  int it = 0;
+  double res = 0.0;
+  bool converged = false;
+  if (bnorm == 0.0) {
+    CUDA_TRY(cudaMemsetAsync(x, 0, N * 8, st));
+    converged = true;
+  }
+  int restarts = 0;
+  while (!converged && it < opts->max_iter) {
+    // (re)start from the true residual: r = b - A x, z = M r, p = z
+    if ((rc = apply(x, G.q))) return rc;
+    k_resid<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.b, G.q, G.r);
+    k_mul_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.Minv, G.r, G.z0);
+    k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, G.z0, 0.0, G.p);
+    if ((rc = dot2(G.r, G.z0, G.r, G.r, d2))) return rc;
+    res = std::sqrt(d2[1]) / bnorm;
+    if (res < opts->tol) { converged = true; break; }
+    if (++restarts > 4) return fail(SOD_GPU_ESTAGNATE, "pressure solve made no progress");
+    double rz = d2[0];
+    while (it < opts->max_iter) {
+      if ((rc = apply(G.p, G.q))) return rc;
+      if ((rc = dot2(G.p, G.q, G.p, G.q, d2))) return rc;
+      if (!(d2[0] > 0.0)) break;  // loss of positivity: restart from the true residual
+      const double alpha = rz / d2[0];
+      k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, alpha, G.p, 1.0, x);
+      k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, -alpha, G.q, 1.0, G.r);
+      k_mul_w<<<nb, 256, 0, st>>>(nw, c->lpoin_w, G.Minv, G.r, G.z0);
+      if ((rc = dot2(G.r, G.z0, G.r, G.r, d2))) return rc;
+      ++it;
+      if (!std::isfinite(d2[1])) return fail(SOD_GPU_ENONFINITE, "non-finite residual in pressure solve");
+      if (std::sqrt(d2[1]) / bnorm < opts->tol) break;  // certify on the true residual
+      const double beta = d2[0] / rz;
+      rz = d2[0];
+      k_axpby<double><<<nb, 256, 0, st>>>(nw, c->lpoin_w, 1.0, G.z0, beta, G.p);
+    }
+  }
+  CUDA_TRY(cudaEventRecord(e1, st));
+  CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (stats) {
+    stats->iterations = it;
+    stats->fallback = 0;
+    stats->res_rel = res;
+    stats->seconds = ms * 1e-3;
+  }
+  if (!converged) return fail(SOD_GPU_ESTAGNATE, "pressure solve did not reach the tolerance");
+  return c->finish();
+}
+
 }  // namespace
 
 extern "C" {
@@ -1174,8 +1302,12 @@ extern "C" {
 int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const sod_solve_opts_t *opts,
                            sod_solve_stats_t *stats) {
   if (!c || !b_in || !x || !opts || opts->max_iter < 1 || !(opts->tol > 0)) return fail(SOD_GPU_EINVAL, "bad argument");
-  if (int prc = no_partition(c, "sod_gpu_pressure_solve")) return prc;
   if (opts->precond != 0 && opts->precond != 1) return fail(SOD_GPU_EINVAL, "precond must be 0 or 1");
+  if (c->halo.on) {
+    if (opts->precond != 0)
+      return fail(SOD_GPU_EINVAL, "the learned preconditioner is not available with a halo plan");
+    return pressure_solve_parts(c, b_in, x, opts, stats);
+  }
   int rc;
   if ((rc = ensure_diag(c)) || (rc = ensure_cg64(c)) || (rc = ensure_cg_loop(c))) return rc;
   auto &G = c->cg;
@@ -2790,9 +2922,10 @@ int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *c, int *iters, double *res_rel) {
 
 int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats) {
   if (!c || !c->inc.ready || !opts || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
-  // a partitioned mesh runs the reference's FP32 pressure solve (precond 2)
-  if (opts->precond != 2)
-    if (int prc = no_partition(c, "sod_gpu_incomp_step with the FP64-certified solve")) return prc;
+  // a partitioned mesh runs the reference's FP32 solve (precond 2) or the
+  // FP64-certified Jacobi solve (precond 0)
+  if (opts->precond == 1)
+    if (int prc = no_partition(c, "sod_gpu_incomp_step with the learned preconditioner")) return prc;
   auto &I = c->inc;
   const long long N = c->npoin;
   const int nw = c->npoin_w;
