@@ -446,8 +446,8 @@ int sod_gpu_comp_get_state(sod_gpu_ctx *ctx, float *rho, float *q, float *E, flo
 /* ---- allocation-free analysis integrals ---------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a solver whose device memory belongs to its own pool or is
- * capped, code running during CUDA-graph stream capture, callers that must
- * not let cudaMalloc synchronise the device inside the time loop), this
+ * capped, callers that must not let cudaMalloc synchronise the device
+ * inside the time loop), this
  * computes the same integrals as sod_gpu_comp_analysis without a context:
  * every input is a device pointer in the reference layout (connec, lpoin_w
  * 1-based; He(3,3,ngaus,nelem), gpvol, dlxigp_ip, Ngp (may be NULL), rho,

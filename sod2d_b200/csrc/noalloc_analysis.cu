@@ -2,9 +2,8 @@
 // eps_T, max Mach) for callers that cannot allocate device memory.
 //
 // Who needs it: a Fortran/OpenACC solver that hands all device memory to
-// its own pool (or runs with a memory cap), code running while a stream is
-// being captured into a CUDA graph, and embedded callers that must not
-// trigger cudaMalloc's implicit device synchronisation inside the time
+// its own pool (or runs with a memory cap), and embedded callers that must
+// not trigger cudaMalloc's implicit device synchronisation inside the time
 // loop.  The context-based sod_gpu_comp_analysis needs a sod_gpu_ctx,
 // whose creation allocates; this entry point takes every array as a plain
 // device pointer in the reference layout and uses a fixed scratch area in a

@@ -1,10 +1,9 @@
 """The allocation-free analysis entry point (sod_gpu_analysis_noalloc).
 
 Callers that cannot allocate device memory -- a solver whose device memory
-belongs to its own pool, code running during CUDA-graph stream capture, or
-callers that must not let cudaMalloc synchronise the device inside the time
-loop -- get the analysis integrals through this entry point, which keeps its
-scratch in a fixed device array.  This test calls it through the C-ABI on
+belongs to its own pool, or callers that must not let cudaMalloc synchronise
+the device inside the time loop -- get the analysis integrals through this
+entry point, which keeps its scratch in a fixed device array.  This test calls it through the C-ABI on
 the state of a short Taylor-Green run and compares it, on two calls in a
 row (the second reuses the scratch the first left behind), with the
 context-based sod_gpu_comp_analysis.  Tolerance: 1e-5 relative, as the
