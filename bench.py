@@ -433,6 +433,59 @@ def workload_config(nelem1d=NELEM_1D):
             "parallelism": "replicas"}
 
 
+def halo_leg(nelem1d=NELEM_1D, nparts=8, steps=5, warmup=3):
+    """The fused RHS on a partitioned mesh: the nelem1d^3 workload split into
+    nparts z-slabs, every part a context with its halo plan (the halo sums
+    of the projections and of the residuals inside sod_gpu_updateF).  The
+    parts run as host threads of one process on ONE device and exchange
+    through LocalHaloGroup, so the wall time here serialises the parts and
+    includes host barriers: it is not a multi-GPU number.  The leg is for
+    the kernel launch list (the halo pack and sum kernels beside the element
+    kernels at a realistic part size) and reports the exchange volume."""
+    import torch
+    from sod2d_b200 import gpu, partition
+    from sod2d_b200.halo import LocalHaloGroup
+    m, ic, rho, q, E, mu_e, u, csound = build_workload(nelem1d)
+    N, n = m.npoin, m.nnode
+    parts = partition.split(m, partition.partition_elements(m, (1, 1, nparts)))
+    group = LocalHaloGroup([p.plan for p in parts], timeout=300.0)
+    dv = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    loc = lambda a, k, nd: np.asarray(a).reshape(k, N)[:, nd].reshape(-1)
+    jobs, ctxs = [], []
+    for p in parts:
+        ctx = gpu.Context(p.mesh, gpu.phys_from_ic(ic))
+        ctx.set_halo(p.plan, group)
+        ctxs.append(ctx)
+        nd, el = p.nodes, p.elems
+        d = [dv(loc(rho, 1, nd)), dv(loc(q, 3, nd)), dv(loc(E, 1, nd)), dv(mu_e.reshape(n, -1)[:, el].reshape(-1))]
+        uu, cs = dv(loc(u, 3, nd)), dv(loc(csound, 1, nd))
+        tau = torch.zeros(p.mesh.nelem, device="cuda")
+        ctx.call("sod_gpu_comp_tau", gpu.dptr(cs), gpu.dptr(uu), gpu.dptr(tau))
+        out = [torch.zeros(k * p.mesh.npoin, device="cuda") for k in (1, 3, 1)]
+
+        def job(ctx=ctx, d=d, tau=tau, out=out, k=0):
+            for _ in range(k):
+                ctx.call("sod_gpu_updateF", *(gpu.dptr(x) for x in d), float(ic.mu_factor), gpu.dptr(tau),
+                         *(gpu.dptr(x) for x in out), None, None, None, None)
+        jobs.append(job)
+    group.run([lambda j=j: j(k=warmup) for j in jobs])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    group.run([lambda j=j: j(k=steps) for j in jobs])
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / steps * 1e3
+    for c in ctxs:
+        c.close()
+    entries = [p.plan.numNodesToComm for p in parts]
+    return {"workload": f"fused RHS, {nelem1d}^3 HEX64 (p=3) split into {nparts} z-slabs, parts as host threads "
+                        f"on one device (LocalHaloGroup)",
+            "shared_entries_per_part": [min(entries), max(entries)],
+            "exchange_bytes_per_rhs_per_part": int(max(entries) * (12 + 5) * 4),
+            "wall_ms_per_rhs_all_parts_serialised": round(wall, 3), "steps": steps,
+            "note": "one device: the parts' kernels run one after another and the exchanges are host-side "
+                    "copies behind barriers; the launch list, not this time, is what this leg is for"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -456,6 +509,8 @@ def main():
                     help="run only the FP32/FP64 precision study against the FP64 oracle (prints its JSON object)")
     ap.add_argument("--ps-nelem1d", type=int, default=16)
     ap.add_argument("--ps-steps", type=int, default=200)
+    ap.add_argument("--halo-split", type=int, default=0,
+                    help="run only the partitioned-RHS leg with this many z-slabs on one device (prints its JSON object)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     pkw = dict(nelem1d=args.p_nelem1d, harvest_steps=args.p_harvest, compare_steps=args.p_compare,
@@ -471,6 +526,13 @@ def main():
             import torch
             torch.cuda.set_device(local)
             print(json.dumps({"precision_study": precision_study(args.ps_nelem1d, args.ps_steps)}))
+        return 0
+    if args.halo_split > 0:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps({"halo_split": halo_leg(args.nelem1d, args.halo_split, steps=min(args.steps, 5),
+                                                     warmup=args.warmup)}))
         return 0
     if args.pressure_only:
         if rank == 0:
