@@ -35,39 +35,53 @@ struct HaloViewT {
 };
 using HaloView = HaloViewT<float>;
 
-template <class T>
+// W > 0: the exchange width as a compile-time constant (the loops over the
+// components unroll, so their loads are issued together); W = 0: v.width at
+// run time.
+template <class T, int W>
 __global__ void k_halo_pack(int nsend, const int *__restrict__ node, HaloViewT<T> v, T *__restrict__ buf) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= nsend) return;
+  constexpr int MW = W > 0 ? W : HALO_MAX_WIDTH;
+  const int width = W > 0 ? W : v.width;
   const long long p = (long long)node[j] * v.nstride;
-  T val[HALO_MAX_WIDTH];
+  T val[MW];
 #pragma unroll
-  for (int k = 0; k < HALO_MAX_WIDTH; ++k)
-    if (k < v.width) val[k] = v.comp[k][p];
+  for (int k = 0; k < MW; ++k)
+    if (k < width) val[k] = v.comp[k][p];
 #pragma unroll
-  for (int k = 0; k < HALO_MAX_WIDTH; ++k)
-    if (k < v.width) buf[(long long)j * v.width + k] = val[k];
+  for (int k = 0; k < MW; ++k)
+    if (k < width) buf[(long long)j * width + k] = val[k];
 }
 
 // For shared node u: contributions ptr[u]..ptr[u+1]-1 in ascending rank
 // order; src < 0 is this rank's own value, else a position in recv.
-template <class T>
+template <class T, int W>
 __global__ void k_halo_sum(int nuniq, const int *__restrict__ uniq_node, const int *__restrict__ ptr,
                            const int *__restrict__ src, HaloViewT<T> v, const T *__restrict__ recv) {
   const int u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= nuniq) return;
+  constexpr int MW = W > 0 ? W : HALO_MAX_WIDTH;
+  const int width = W > 0 ? W : v.width;
   const long long p = (long long)uniq_node[u] * v.nstride;
   const int b = ptr[u], e = ptr[u + 1];
-  for (int k = 0; k < v.width; ++k) {
-    const T own = v.comp[k][p];
-    T acc = 0;
-    for (int i = b; i < e; ++i) {
-      const int s = src[i];
-      const T x = s < 0 ? own : recv[(long long)s * v.width + k];
-      acc = i == b ? x : acc + x;
-    }
-    v.comp[k][p] = acc;
+  T own[MW], acc[MW];
+#pragma unroll
+  for (int k = 0; k < MW; ++k)
+    if (k < width) own[k] = v.comp[k][p];
+  for (int i = b; i < e; ++i) {
+    const int s = src[i];
+    T x[MW];
+#pragma unroll
+    for (int k = 0; k < MW; ++k)
+      if (k < width) x[k] = s < 0 ? own[k] : recv[(long long)s * width + k];
+#pragma unroll
+    for (int k = 0; k < MW; ++k)
+      if (k < width) acc[k] = i == b ? x[k] : acc[k] + x[k];
   }
+#pragma unroll
+  for (int k = 0; k < MW; ++k)
+    if (k < width) v.comp[k][p] = acc[k];
 }
 
 }  // namespace

@@ -17,6 +17,7 @@
 #include <vector>
 #include <map>
 #include <algorithm>
+#include <type_traits>
 #include <array>
 #include <cmath>
 #include <random>
@@ -330,15 +331,31 @@ int halo_sum(sod_gpu_ctx *c, const HaloViewT<T> &v) {
   static_assert(sizeof(T) % sizeof(float) == 0, "values travel as whole floats");
   if ((int)(v.width * sizeof(T) / sizeof(float)) > HALO_MAX_WIDTH)
     return fail(SOD_GPU_EINVAL, "halo exchange wider than the buffers");
-  if (h.nsend > 0)
-    k_halo_pack<T><<<nblk(h.nsend, 256), 256, 0, c->stream>>>(h.nsend, h.send_node, v, (T *)h.send);
+  // the widths the library exchanges get their own instantiation
+  auto launch = [&](auto wc, bool pack) {
+    constexpr int W = decltype(wc)::value;
+    if (pack)
+      k_halo_pack<T, W><<<nblk(h.nsend, 256), 256, 0, c->stream>>>(h.nsend, h.send_node, v, (T *)h.send);
+    else
+      k_halo_sum<T, W><<<nblk(h.nuniq, 128), 128, 0, c->stream>>>(h.nuniq, h.uniq_node, h.ptr, h.src, v,
+                                                                  (const T *)h.recv);
+  };
+  auto by_width = [&](bool pack) {
+    switch (v.width) {
+      case 12: launch(std::integral_constant<int, 12>{}, pack); break;
+      case 6: launch(std::integral_constant<int, 6>{}, pack); break;
+      case 5: launch(std::integral_constant<int, 5>{}, pack); break;
+      case 3: launch(std::integral_constant<int, 3>{}, pack); break;
+      case 1: launch(std::integral_constant<int, 1>{}, pack); break;
+      default: launch(std::integral_constant<int, 0>{}, pack); break;
+    }
+  };
+  if (h.nsend > 0) by_width(true);
   CUDA_TRY(cudaGetLastError());
   const int width_floats = v.width * (int)(sizeof(T) / sizeof(float));
   if (h.fn(h.user, h.send, h.recv, width_floats, (void *)c->stream) != 0)
     return fail(SOD_GPU_EINVAL, "halo exchange callback failed");
-  if (h.nuniq > 0)
-    k_halo_sum<T><<<nblk(h.nuniq, 128), 128, 0, c->stream>>>(h.nuniq, h.uniq_node, h.ptr, h.src, v,
-                                                             (const T *)h.recv);
+  if (h.nuniq > 0) by_width(false);
   CUDA_TRY(cudaGetLastError());
   return 0;
 }
