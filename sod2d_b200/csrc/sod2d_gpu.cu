@@ -207,14 +207,26 @@ __global__ void k_lumped(int npoin_w, long long npoin, const int *__restrict__ l
   for (int c = 0; c < ncomp; ++c) R[p + npoin * c] = R[p + npoin * c] * a;
 }
 
-// Reference-layout field (nelem, nnode) -> internal [e][t].
-__global__ void k_elem_to_t(long long nelem, int N, const int *__restrict__ a_of_t,
-                            const float *__restrict__ src, float *__restrict__ dst) {
-  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= nelem * N) return;
-  long long e = idx / N;
-  int t = (int)(idx % N);
-  dst[idx] = src[e + nelem * a_of_t[t]];
+// Reference-layout field (nelem, nnode) -> internal [e][t], as a tiled
+// transpose: a block takes 32 consecutive elements, reads each node's 32
+// values as one coalesced row (the reference layout is element-fastest)
+// into shared memory and writes the 32 elements' N values contiguously.
+constexpr int E2T_TILE = 32;
+constexpr int E2T_THREADS = 256;
+__global__ void __launch_bounds__(E2T_THREADS) k_elem_to_t(long long nelem, int N, const int *__restrict__ a_of_t,
+                                                           const float *__restrict__ src, float *__restrict__ dst) {
+  __shared__ float tile[125][E2T_TILE + 1];  // N <= 125 (P = 4)
+  const long long e0 = (long long)blockIdx.x * E2T_TILE;
+  const int tx = threadIdx.x % E2T_TILE, ty = threadIdx.x / E2T_TILE;
+  constexpr int ROWS = E2T_THREADS / E2T_TILE;
+  const long long e = e0 + tx;
+  for (int a = ty; a < N; a += ROWS) tile[a][tx] = e < nelem ? src[e + nelem * a] : 0.f;
+  __syncthreads();
+  const long long ne = nelem - e0 < E2T_TILE ? nelem - e0 : E2T_TILE;
+  for (int f = threadIdx.x; f < ne * N; f += E2T_THREADS) {
+    const int le = f / N, t = f % N;
+    dst[(e0 + le) * N + t] = tile[a_of_t[t]][le];
+  }
 }
 
 // Internal [e][t] -> reference-layout (nelem, nnode).
@@ -736,13 +748,13 @@ int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
       !ProjMZ || !tau_stab || !Rmass || !Rmom || !Rener)
     return fail(SOD_GPU_EINVAL, "bad argument");
   const long long EN = (long long)c->nelem * c->N;
-  k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
+  k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   if (mu_sgs) {
     if (!c->musgs_t) {
       int rc = c->alloc(&c->musgs_t, (size_t)EN);
       if (rc) return rc;
     }
-    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+    k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
   }
   k_pack_proj<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, ProjMX, ProjMY, ProjMZ, ProjMass, ProjEner,
                                                           c->proj12);
@@ -769,13 +781,13 @@ int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
   if (!c || !rho_n || !rho || !u || !Tem || !mu_fluid || !mu_e || !Rmass || !Rmom || !Rener)
     return fail(SOD_GPU_EINVAL, "bad argument");
   const long long EN = (long long)c->nelem * c->N;
-  k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
+  k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   if (mu_sgs) {
     if (!c->musgs_t) {
       int rc = c->alloc(&c->musgs_t, (size_t)EN);
       if (rc) return rc;
     }
-    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+    k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
   }
   RhsArgs A{};
   A.rho = rho; A.u = u; A.Tem = Tem; A.mu_fluid = mu_fluid;
@@ -797,7 +809,7 @@ int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
 int sod_gpu_set_mu_e(sod_gpu_ctx *c, const float *mu_e) {
   if (!c || !mu_e) return fail(SOD_GPU_EINVAL, "bad argument");
   const long long EN = (long long)c->nelem * c->N;
-  k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
+  k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   c->mue_set = true;
   return c->finish();
 }
@@ -809,7 +821,7 @@ int sod_gpu_updateF(sod_gpu_ctx *c, const float *rho, const float *q, const floa
     return fail(SOD_GPU_EINVAL, "bad argument");
   if (!mu_e && !c->mue_set) return fail(SOD_GPU_EINVAL, "mu_e is NULL and sod_gpu_set_mu_e was not called");
   const long long EN = (long long)c->nelem * c->N;
-  if (mu_e) k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
+  if (mu_e) k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_e, c->mue_t);
   RhsArgs A{};
   A.rho = rho; A.q = q; A.E = E; A.mu_factor = mu_factor;
   A.mue_t = c->mue_t; A.tau_stab = tau_stab; A.proj12 = c->proj12;
@@ -2816,7 +2828,7 @@ int sod_gpu_full_diff_stab_incomp(sod_gpu_ctx *c, const float *u, const float *m
   const long long EN = (long long)c->nelem * c->N;
   if (mu_sgs) {
     if (!c->musgs_t && (rc = c->alloc(&c->musgs_t, (size_t)EN))) return rc;
-    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+    k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
   }
   k_pack_tauv<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->npoin, TauPX, TauPY, TauPZ, c->velo.tauP);
   velo_diff(c, u, mu_fluid, mu_sgs ? c->musgs_t : nullptr, tau_stab, Rmom);
@@ -2838,7 +2850,7 @@ int sod_gpu_conjgrad_veloc(sod_gpu_ctx *c, float fact, float dt, const float *mu
   const float *musgs = nullptr;
   if (mu_sgs) {
     if (!c->musgs_t && (rc = c->alloc(&c->musgs_t, (size_t)EN))) return rc;
-    k_elem_to_t<<<nblk(EN, 256), 256, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
+    k_elem_to_t<<<nblk(c->nelem, E2T_TILE), E2T_THREADS, 0, c->stream>>>(c->nelem, c->N, c->a_of_t, mu_sgs, c->musgs_t);
     musgs = c->musgs_t;
   }
   CUDA_TRY(cudaMemcpyAsync(V.x, Rp0, 3 * N * 4, cudaMemcpyDeviceToDevice, c->stream));
