@@ -1701,7 +1701,7 @@ int comp_visc(sod_gpu_ctx *c, const float *Reta, const float *rho, const float *
   auto &S = c->comp;
   const unsigned init_bits = 0x47C35000u;  // 100000.0f
   CUDA_TRY(cudaMemcpyAsync(S.bits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
-  k_min_rho<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, S.bits);
+  k_min_rho<<<MINMAX_BLOCKS, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, S.bits);
   // the bits of a positive float order like the float: reduce as float
   int rc = allreduce(c, S.bits, 1, SOD_REDUCE_MIN_F32);
   if (rc) return rc;
@@ -1746,7 +1746,7 @@ int sod_gpu_smart_visc_spectral_imex(sod_gpu_ctx *c, const float *Reta, const fl
   if (!c->vbits && (rc = c->alloc(&c->vbits, 4))) return rc;
   const unsigned init_bits = 0x47C35000u;  // 100000.0f, the reference's initial minimum
   CUDA_TRY(cudaMemcpyAsync(c->vbits, &init_bits, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
-  k_min_rho<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, c->vbits);
+  k_min_rho<<<MINMAX_BLOCKS, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, rho, c->vbits);
   if ((rc = allreduce(c, c->vbits, 1, SOD_REDUCE_MIN_F32))) return rc;
   ViscArgs V{};
   V.Reta = Reta; V.rho = rho; V.u = u; V.csound = csound; V.Ml = c->Ml;
@@ -2209,7 +2209,7 @@ int sod_gpu_comp_analysis(sod_gpu_ctx *c, float rho0, double *out) {
   k_sum_parts<<<1, 1024, 0, c->stream>>>(c->nelem, S.part, S.sums);
   const unsigned zero = 0u;
   CUDA_TRY(cudaMemcpyAsync(S.bits + 2, &zero, 4, cudaMemcpyHostToDevice, c->stream));
-  k_max_mach<<<296, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, S.machno, S.bits + 2);
+  k_max_mach<<<MINMAX_BLOCKS, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, S.machno, S.bits + 2);
   int rc;
   if ((rc = allreduce(c, S.sums, 3, SOD_REDUCE_SUM_F64)) || (rc = allreduce(c, S.bits + 2, 1, SOD_REDUCE_MAX_F32)))
     return rc;

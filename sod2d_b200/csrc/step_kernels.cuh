@@ -214,11 +214,25 @@ __global__ void k_aux_reta(int npoin_w, const int *__restrict__ lpoin_w, float d
 }
 
 // Minimum of rho over working nodes (order-independent, deterministic).
+// grid of the node min / max reductions: 8 blocks of 256 per SM
+constexpr int MINMAX_BLOCKS = 148 * 8;
 __global__ void k_min_rho(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ rho,
                           unsigned int *__restrict__ out_bits) {
   float v = 100000.0f;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npoin_w; t += gridDim.x * blockDim.x)
-    v = fminf(v, rho[lpoin_w[t]]);
+  // four strides per trip with every load issued first (min is order-free)
+  const int stride = gridDim.x * blockDim.x;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t + 3 * stride < npoin_w; t += 4 * stride) {
+    int p[4];
+    float x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) p[u] = lpoin_w[t + u * stride];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = rho[p[u]];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v = fminf(v, x[u]);
+  }
+  for (; t < npoin_w; t += stride) v = fminf(v, rho[lpoin_w[t]]);
   for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) atomicMin(out_bits, __float_as_uint(v));  // rho > 0: bit order = value order
 }
@@ -468,8 +482,19 @@ __global__ void k_sum_parts(long long nelem, const float *__restrict__ part, dou
 __global__ void k_max_mach(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ machno,
                            unsigned int *__restrict__ out_bits) {
   float v = 0.f;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npoin_w; t += gridDim.x * blockDim.x)
-    v = fmaxf(v, machno[lpoin_w[t]]);
+  const int stride = gridDim.x * blockDim.x;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (; t + 3 * stride < npoin_w; t += 4 * stride) {
+    int p[4];
+    float x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) p[u] = lpoin_w[t + u * stride];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = machno[p[u]];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) v = fmaxf(v, x[u]);
+  }
+  for (; t < npoin_w; t += stride) v = fmaxf(v, machno[lpoin_w[t]]);
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out_bits, __float_as_uint(v));
 }
