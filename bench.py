@@ -42,8 +42,7 @@ sys.path.insert(0, str(ROOT))
 B_PER_NODE_STAGE = 402.0
 # DRAM bytes (read + write) of one RHS evaluation per working node, from one
 # ncu capture of the four RHS kernels on the 32^3 workload (548,663,296 B for
-# 884,736 working nodes; profiles/rhs_kernels_64cube_p3.md), scaled by the
-# working nodes of the benchmarked mesh.
+# 884,736 working nodes), scaled by the working nodes of the benchmarked mesh.
 DRAM_B_PER_NODE_STAGE = 548663296 / 884736
 NELEM_1D = 64
 PORDER = 3
@@ -164,17 +163,16 @@ def build_workload(nelem_1d: int, seed: int = 2024):
 
 
 class CpuBaseline:
-    """The oracle's FP32 RHS (OpenMP over all host cores) on a bounded sample
-    of the workload: a 32^3-element jittered cube of the same order (884,736
-    working nodes)."""
+    """The oracle's FP32 RHS (OpenMP over all host cores) on the benchmarked
+    workload itself (the same nelem1d^3 jittered cube and state); a bounded
+    number of whole-mesh evaluations is timed."""
 
-    NELEM_1D = 32
-
-    def __init__(self):
+    def __init__(self, nelem1d=NELEM_1D):
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
         self.O = O
-        m, ic, rho, q, E, mu_e, u, csound = build_workload(self.NELEM_1D)
+        self.NELEM_1D = nelem1d
+        m, ic, rho, q, E, mu_e, u, csound = build_workload(nelem1d)
         self.m, self.ic, self.args = m, ic, (rho, q, E, mu_e)
         self.om = O.OracleMesh(m)
         self.tau = O.comp_tau(self.om, csound, u)
@@ -202,7 +200,7 @@ class CpuBaseline:
 def run_reference(args, rank, world):
     if rank != 0:
         return 0
-    cb = CpuBaseline()
+    cb = CpuBaseline(args.nelem1d)
     for _ in range(args.warmup):
         cb.step()
     times = [cb.step() for _ in range(args.steps)]
@@ -705,7 +703,7 @@ def main():
         line["imex_step"] = imex_step_leg(args.nelem1d)
         line["pressure_solve"] = pressure_leg(**pkw)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = CpuBaseline().sample()
+        line["cpu_baseline"] = CpuBaseline(args.nelem1d).sample()
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -456,11 +456,12 @@ int sod_gpu_comp_get_state(sod_gpu_ctx *ctx, float *rho, float *q, float *E, flo
  * It allocates nothing: its scratch is a fixed __device__ array of
  * SOD_NOALLOC_MAX_ELEM x 3 floats (12 MiB) that each GPU loading the
  * library keeps until the process exits; larger meshes are rejected with
- * SOD_GPU_EINVAL.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU
- * race; serialise them.  Work is enqueued on `stream` (NULL = default) and
- * the call returns after the results have been copied to out. */
+ * SOD_GPU_EINVAL.  Every call looks up the array's device address in the
+ * current context (cudaGetSymbolAddress; the first call in a context also
+ * loads the library's device code there).  All calls share the array, so
+ * calls that overlap on the GPU race; serialise them.  Work is enqueued on
+ * `stream` (NULL = default); the call copies the results into the host
+ * array out and waits on `stream` for them before it returns. */
 #define SOD_NOALLOC_MAX_ELEM (1 << 20)
 int sod_gpu_analysis_noalloc(int porder, int nelem, int npoin, int npoin_w, const int *connec,
                              const int *lpoin_w, const int *invAtoIJK, const int *gmshAtoI,

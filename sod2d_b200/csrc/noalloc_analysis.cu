@@ -21,7 +21,6 @@
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 int sod_detail_set_error(int code, const char *msg);  // sod2d_gpu.cu
 
@@ -35,20 +34,16 @@ constexpr size_t kScratchBytes = kPartBytes + 4 * sizeof(double);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch per device, resolved once per device.
-std::mutex g_mu;
-void *g_addr[64] = {nullptr};
-
+// Device address of g_noalloc_scratch in the calling thread's current
+// context.  Looked up on every call (a table lookup in the runtime once the
+// module is loaded; the first call in a context also loads the module
+// there): a cached address would go stale after cudaDeviceReset or when the
+// caller switches to another context on the same device, and the kernels
+// would then write through a dangling pointer.
 int scratch_address(void **out) {
-  int dev = -1;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
-  std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return -1;
-    g_addr[dev] = p;
-  }
-  *out = g_addr[dev];
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return -1;
+  *out = p;
   return 0;
 }
 

@@ -21,7 +21,9 @@ SOURCES = {
 }
 
 if __name__ == "__main__":
-    root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <root of the reference checkout>")
+    root = Path(sys.argv[1])
     here = Path(__file__).resolve().parent
     for dst, src in SOURCES.items():
         shutil.copyfile(root / src, here / dst)

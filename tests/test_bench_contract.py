@@ -1,6 +1,7 @@
 """The reference arm of bench.py (the oracle's FP32 RHS on the host cores)
 runs without a GPU: its single JSON line carries the keys of the bench
-contract, with a cpu_baseline and an e2e object describing the run."""
+contract, with a cpu_baseline and an e2e object describing the run, and its
+config names the mesh that was timed."""
 import json
 import subprocess
 import sys
@@ -10,7 +11,8 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def test_reference_arm_json_line():
-    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1"],
+    p = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1",
+                        "--nelem1d", "16"],
                        cwd=ROOT, capture_output=True, text=True, timeout=900)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [l for l in p.stdout.strip().splitlines() if l.startswith("{")]
@@ -22,7 +24,9 @@ def test_reference_arm_json_line():
     # the bench runs at least 3 warm-up steps whatever is asked, and reports them
     assert d["impl"] == "reference" and d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1
     assert d["value"] > 0 and d["higher_is_better"] is True
-    assert "workload" in d["config"] and d["config"]["working_nodes"] > 0
+    # the config describes what was timed: the 16^3 cube asked for
+    assert "workload" in d["config"] and d["config"]["working_nodes"] == 48 ** 3
+    assert "16^3" in d["config"]["workload"] and "16^3" in d["cpu_baseline"]["sample"]
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     e2e = d["e2e"]

@@ -3,11 +3,13 @@
 Callers that cannot allocate device memory -- a solver whose device memory
 belongs to its own pool, or callers that must not let cudaMalloc synchronise
 the device inside the time loop -- get the analysis integrals through this
-entry point, which keeps its scratch in a fixed device array.  This test calls it through the C-ABI on
-the state of a short Taylor-Green run and compares it, on two calls in a
-row (the second reuses the scratch the first left behind), with the
-context-based sod_gpu_comp_analysis.  Tolerance: 1e-5 relative, as the
-other FP32 parity tests.  It sits in a file of its own, collected last.
+entry point, which keeps its scratch in a fixed device array.  This test
+calls it through the C-ABI on the state of a short Taylor-Green run, for
+element orders 3 and 4, and compares it, on two calls in a row (the second
+reuses the scratch the first left behind), with the context-based
+sod_gpu_comp_analysis.  Tolerance: 1e-5 relative, as the other FP32 parity
+tests.  The free device memory after the second call equals that after the
+first: the call allocates nothing.  The file is collected last.
 """
 import ctypes as C
 
@@ -30,8 +32,9 @@ def gpu():
     return g
 
 
-def test_noalloc_analysis_matches_context_entry_point(gpu):
-    m = host.periodic_cube(3, 6, jitter=0.05, seed=21, ordering=1)
+@pytest.mark.parametrize("porder,nelem1d", [(3, 6), (4, 4)])
+def test_noalloc_analysis_matches_context_entry_point(gpu, porder, nelem1d):
+    m = host.periodic_cube(porder, nelem1d, jitter=0.05, seed=21, ordering=1)
     ic = host.tgv_comp_init(m, Ma=0.1)
     s = gpu.CompSolver(m, ic, stages=4, fp64_state=False)
     for _ in range(3):  # non-zero entropy viscosity
@@ -59,6 +62,7 @@ def test_noalloc_analysis_matches_context_entry_point(gpu):
                                          "dlxigp_ip", "He", "gpvol", "Ngp")}
     fields = {k: dv(v) for k, v in dict(rho=rho, u=u.reshape(-1), mu=mu, mu_e=st["mu_e"], machno=machno).items()}
     volT = float(np.float32(m.vol_total))
+    torch.cuda.synchronize()
 
     def call(nelem=m.nelem):
         out = (C.c_double * 5)()
@@ -70,12 +74,17 @@ def test_noalloc_analysis_matches_context_entry_point(gpu):
             float(ic.rho0), volT, None, out)
         return rc, np.array(out[:])
 
+    free_after = []
     for attempt in range(2):  # two calls in a row share the scratch
         rc, got = call()
         assert rc == 0, gpu.lib().sod_gpu_last_error()
+        free_after.append(torch.cuda.mem_get_info()[0])
         rel = np.abs(got - ref) / np.abs(ref)
-        print(f"call {attempt}: rel diff {rel}")
+        print(f"p={porder} call {attempt}: rel diff {rel}")
         assert rel.max() < TOL, (got, ref)
+    # the first call may load the library's device code into this context;
+    # the second finds nothing more to set up and must allocate nothing
+    assert free_after[1] == free_after[0], free_after
 
     # sizes beyond the fixed scratch are rejected with a clear error
     rc, _ = call(nelem=(1 << 20) + 1)
