@@ -263,7 +263,9 @@ typedef struct {
   double tol;
   int precond;         /* 0 Jacobi, 1 learned; 2 (sod_gpu_incomp_step only):
                           the reference's conjGrad_pressure_incomp in FP32
-                          with max_iter / tol, uncertified                 */
+                          with max_iter / tol, uncertified; 3
+                          (sod_gpu_incomp_step only): Jacobi from the
+                          learned path's initial guess 2 p^n - p^(n-1)    */
   int stagnation_window; /* iterations without a 2x residual drop -> fallback */
   int harvest;         /* 1: record (residual, error) pairs of this solve for
                           training the learned preconditioner             */

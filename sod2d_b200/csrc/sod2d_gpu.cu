@@ -56,7 +56,8 @@ struct sod_gpu_ctx {
   Phys ph{};
   sod_phys_t phys{};
   // device mirrors
-  int *conn = nullptr, *lpoin_w = nullptr, *slot_ptr = nullptr, *slot_idx = nullptr, *lelpn = nullptr;
+  int *conn = nullptr, *lpoin_w = nullptr, *slot_ptr = nullptr, *slot_idx = nullptr, *slot_pos = nullptr,
+      *lelpn = nullptr;
   int *a_of_t = nullptr;  // tensor position -> reference local node (0-based)
   float *geo = nullptr, *Dnat = nullptr, *invMl = nullptr, *Ml = nullptr, *helem = nullptr, *helem_l_t = nullptr;
   // scratch
@@ -167,7 +168,7 @@ struct sod_gpu_ctx {
     MeshDev m;
     m.nelem = nelem; m.npoin = npoin; m.npoin_w = npoin_w;
     m.conn = conn; m.geo = geo; m.Dnat = Dnat; m.lpoin_w = lpoin_w; m.invMl = invMl;
-    m.slot_ptr = slot_ptr; m.slot_idx = slot_idx;
+    m.slot_ptr = slot_ptr; m.slot_idx = slot_idx; m.slot_pos = slot_pos;
     return m;
   }
   template <class T>
@@ -299,6 +300,18 @@ __global__ void k_comp_tau(long long nelem, int N, const int *__restrict__ conn,
   if (lane == 0) tau[e] = taul;
 }
 
+int num_sms() {
+  // initialised once, thread-safely (contexts may be driven from several host threads)
+  static const int n = [] {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1)
+      v = 148;
+    return v;
+  }();
+  return n;
+}
+
 inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 
 // ---- launch helpers templated on the element order --------------------
@@ -316,9 +329,21 @@ struct Launch {
     else
       k_proj<P, EPB, false><<<grid(c->nelem), TPB, 0, c->stream>>>(c->md(), c->ph, c->phys.Rgas, a0, a1, a2, c->slotsA);
   }
+  // Persistent pass B: as many blocks as fit on the GPU at once (at most
+  // one per element group), each walking the groups with a stride.
   template <int MODE, int IN>
   static void rhs(sod_gpu_ctx *c, const RhsArgs &A) {
-    k_rhs<P, EPB, MODE, IN><<<grid(c->nelem), TPB, 0, c->stream>>>(c->md(), c->ph, c->phys.Rgas, A, c->slotsB);
+    using PL = RhsPlan<P, EPB, MODE, IN>;
+    static const int per_sm = [] {
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_rhs<P, EPB, MODE, IN>, TPB, PL::BYTES) != cudaSuccess ||
+          nb < 1)
+        nb = 1;
+      return nb;
+    }();
+    const long long groups = grid(c->nelem);
+    const unsigned g = (unsigned)std::min<long long>(groups, (long long)per_sm * num_sms());
+    k_rhs<P, EPB, MODE, IN><<<g, TPB, PL::BYTES, c->stream>>>(c->md(), c->ph, c->phys.Rgas, A, c->slotsB);
   }
 };
 
@@ -418,8 +443,8 @@ void gather_res(sod_gpu_ctx *c, float *Rmass, float *Rmom, float *Rener, int acc
   OutPtrs o{};
   const long long N = c->npoin;
   o.p[0] = Rmass; o.p[1] = Rener; o.p[2] = Rmom; o.p[3] = Rmom + N; o.p[4] = Rmom + 2 * N;
-  k_gather_res5<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, (long long)c->nelem * c->N, o,
-                                                             accumulate, invml);
+  k_gather_sorted_res5<<<nblk(c->npoin, 256), 256, 0, c->stream>>>(c->md(), c->slotsB, (long long)c->nelem * c->N,
+                                                                    o, accumulate, invml);
 }
 
 }  // namespace
@@ -476,9 +501,13 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
       geo[(e * 10 + 9) * N + t] = mesh->gpvol[a + (long long)N * e];
     }
   for (long long p = 0; p < NP; ++p) cnt[p + 1] += cnt[p];
-  std::vector<int> slot_idx((size_t)E * N), fillp(cnt.begin(), cnt.end() - 1);
+  std::vector<int> slot_idx((size_t)E * N), slot_pos((size_t)E * N), fillp(cnt.begin(), cnt.end() - 1);
   for (long long e = 0; e < E; ++e)
-    for (int t = 0; t < N; ++t) slot_idx[fillp[conn[e * N + t]]++] = (int)(e * N + t);
+    for (int t = 0; t < N; ++t) {
+      const int s = fillp[conn[e * N + t]]++;
+      slot_idx[s] = (int)(e * N + t);
+      slot_pos[e * N + t] = s;
+    }
   std::vector<int> lw(mesh->npoin_w);
   for (int t = 0; t < mesh->npoin_w; ++t) {
     lw[t] = mesh->lpoin_w[t] - 1;
@@ -499,6 +528,7 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
       (rc = c->upload(&c->Dnat, D.data(), D.size())) || (rc = c->upload(&c->lpoin_w, lw.data(), lw.size())) ||
       (rc = c->upload(&c->slot_ptr, cnt.data(), cnt.size())) ||
       (rc = c->upload(&c->slot_idx, slot_idx.data(), slot_idx.size())) ||
+      (rc = c->upload(&c->slot_pos, slot_pos.data(), slot_pos.size())) ||
       (rc = c->upload(&c->invMl, mesh->invMl, (size_t)NP)) || (rc = c->upload(&c->Ml, mesh->Ml, (size_t)NP)) ||
       (rc = c->upload(&c->a_of_t, a_of_t.data(), a_of_t.size())) ||
       (rc = c->alloc(&c->slotsA, (size_t)E * N * 12)) || (rc = c->alloc(&c->slotsB, (size_t)E * N * 8)) ||
@@ -763,7 +793,7 @@ int sod_gpu_full_diff_stab_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
   A.mue_t = c->mue_t; A.musgs_t = mu_sgs ? c->musgs_t : nullptr; A.tau_stab = tau_stab; A.proj12 = c->proj12;
   A.fact_d = fact;
   Phys saved = c->ph;
-  c->ph.Cp = Cp; c->ph.Prt = Pr;
+  c->ph.Cp = Cp; c->ph.Prt = Pr; c->ph.cp_pr = Cp / Pr;
   int rc = dispatch(c, [&](auto L) {
     L.template rhs<MODE_DIFF, IN_DIFF>(c, A);
     return 0;
@@ -795,7 +825,7 @@ int sod_gpu_full_diffusion_ijk(sod_gpu_ctx *c, float Cp, float Pr, const float *
   A.mue_t = c->mue_t; A.musgs_t = mu_sgs ? c->musgs_t : nullptr;
   A.fact_d = fact;
   Phys saved = c->ph;
-  c->ph.Cp = Cp; c->ph.Prt = Pr;
+  c->ph.Cp = Cp; c->ph.Prt = Pr; c->ph.cp_pr = Cp / Pr;
   int rc = dispatch(c, [&](auto L) {
     L.template rhs<MODE_DIFF | MODE_NOLPS, IN_DIFF>(c, A);
     return 0;
@@ -955,17 +985,6 @@ int ensure_cg64(sod_gpu_ctx *c) {
 
 constexpr int CG_HIST = 1024;
 
-int num_sms() {
-  // initialised once, thread-safely (contexts may be driven from several host threads)
-  static const int n = [] {
-    int dev = 0, v = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1)
-      v = 148;
-    return v;
-  }();
-  return n;
-}
 
 // grid of the tensor-core patch kernel: one block per SM (the block's
 // registers and shared memory allow one), fewer when there are fewer
@@ -2951,8 +2970,9 @@ int sod_gpu_incomp_veloc_stats(sod_gpu_ctx *c, int *iters, double *res_rel) {
 
 int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, sod_solve_stats_t *stats) {
   if (!c || !c->inc.ready || !opts || !(dt > 0.f)) return fail(SOD_GPU_EINVAL, "bad argument");
+  if (opts->precond < 0 || opts->precond > 3) return fail(SOD_GPU_EINVAL, "precond must be 0, 1, 2 or 3");
   // a partitioned mesh runs the reference's FP32 solve (precond 2) or the
-  // FP64-certified Jacobi solve (precond 0)
+  // FP64-certified Jacobi solve (precond 0 or 3)
   if (opts->precond == 1)
     if (int prc = no_partition(c, "sod_gpu_incomp_step with the learned preconditioner")) return prc;
   auto &I = c->inc;
@@ -3005,11 +3025,15 @@ int sod_gpu_incomp_step(sod_gpu_ctx *c, float dt, const sod_solve_opts_t *opts, 
   } else {
     // initial guess: the previous pressure for Jacobi (the reference's
     // pr(:,1), mod_solver_incomp.f90:306); extrapolated from the previous
-    // two pressures for the learned path
-    const int hist = opts->precond == 1 ? I.nsteps : (I.nsteps > 0 ? 1 : 0);
+    // two pressures for the learned path and for precond 3 (Jacobi with the
+    // learned path's guess)
+    const bool extrap = opts->precond == 1 || opts->precond == 3;
+    const int hist = extrap ? I.nsteps : (I.nsteps > 0 ? 1 : 0);
     k_poisson_rhs<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, I.div, k.g0, dt, I.p, I.pold, hist, I.b, I.x);
     c->async = was_async;
-    rc = sod_gpu_pressure_solve(c, I.b, I.x, opts, stats);
+    sod_solve_opts_t o = *opts;
+    if (o.precond == 3) o.precond = 0;
+    rc = sod_gpu_pressure_solve(c, I.b, I.x, &o, stats);
     if (rc && rc != SOD_GPU_ESTAGNATE) return rc;
     solve_rc = rc;
     {  // pold = p; p = x

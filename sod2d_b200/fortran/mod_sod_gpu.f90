@@ -50,7 +50,7 @@ module mod_sod_gpu
    type, bind(C) :: sod_solve_opts_t
       integer(c_int) :: max_iter
       real(c_double) :: tol
-      integer(c_int) :: precond            ! 0 Jacobi, 1 learned, 2 reference FP32 CG
+      integer(c_int) :: precond            ! 0 Jacobi, 1 learned, 2 reference FP32 CG, 3 Jacobi + extrapolated guess
       integer(c_int) :: stagnation_window
       integer(c_int) :: harvest
    end type
