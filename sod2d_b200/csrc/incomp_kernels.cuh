@@ -9,17 +9,30 @@ namespace sod {
 
 // ---- Laplacian: ResP = sum_e int grad N . grad p  (mod_operators.f90:16-112)
 // One thread per Gauss point; V = float (reference arithmetic) or double.
-// Writes one V per element node into slots (width 1).
-template <int P, int EPB, class V>
+// Writes one V per element node into slots (width 1), element-ordered.
+// DIR (the CG iteration): the operand is the new search direction
+// z + beta p, formed on the fly from z, the previous p and *beta (the
+// update p = z + beta p itself is stored by k_cg_q), and the slots are
+// written node-sorted (slot_pos) for k_cg_q's contiguous sums.
+template <int P, int EPB, class V, bool DIR = false>
 __global__ void __launch_bounds__(EPB *Cfg<P>::NT)
-k_lap_elem(MeshDev m, const V *__restrict__ p, V *__restrict__ slots, const int *__restrict__ stop = nullptr) {
+k_lap_elem(MeshDev m, const V *__restrict__ p, V *__restrict__ slots, const int *__restrict__ stop = nullptr,
+           const V *__restrict__ z = nullptr, const V *__restrict__ beta = nullptr) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT;
   if (stop && *stop) return;
   __shared__ V sm[EPB][4][N];
   const int el = threadIdx.x / NT, t = threadIdx.x % NT;
   const long long e = (long long)blockIdx.x * EPB + el;
   const bool active = (e < m.nelem) && (t < N);
-  if (active) sm[el][0][t] = p[m.conn[e * N + t]];
+  if (active) {
+    const int n = m.conn[e * N + t];
+    if (DIR) {
+      const V bt = *beta;
+      sm[el][0][t] = z[n] + bt * p[n];
+    } else {
+      sm[el][0][t] = p[n];
+    }
+  }
   __syncthreads();
   const int i = t % N1, j = (t / N1) % N1, k = t / (N1 * N1);
   V C0 = 0, C1 = 0, C2 = 0;
@@ -62,7 +75,7 @@ k_lap_elem(MeshDev m, const V *__restrict__ p, V *__restrict__ slots, const int 
     acc += (V)m.Dnat[mm * N1 + j] * sm[el][2][i + N1 * mm + N1 * N1 * k];
     acc += (V)m.Dnat[mm * N1 + k] * sm[el][3][i + N1 * j + N1 * N1 * mm];
   }
-  slots[e * N + t] = acc;
+  slots[DIR ? (long long)m.slot_pos[e * N + t] : e * N + t] = acc;
 }
 
 // Scalar-slot assembly out(p) = scale * sum(slots of p); float sums are
@@ -371,12 +384,16 @@ __device__ bool grid_sum(double (&v)[ND], double *__restrict__ part, unsigned *t
 }
 
 // q = assembled Laplacian slots (Kahan, as k_gather1) with the p.q partials;
-// the last block sets alpha = rz / pq.
+// the last block sets alpha = rz / pq.  DIR: the slots are node-sorted
+// (k_lap_elem<DIR>), and the new search direction p = z + beta p is formed
+// and stored here for every node with slots (the working nodes).
+template <bool DIR = false>
 __global__ void __launch_bounds__(CG_THREADS)
-k_cg_q(MeshDev m, const double *__restrict__ slots, const double *__restrict__ p, double *__restrict__ q,
-       CgScal *S, double *__restrict__ part, unsigned *ticket) {
+k_cg_q(MeshDev m, const double *__restrict__ slots, double *__restrict__ p, double *__restrict__ q,
+       CgScal *S, double *__restrict__ part, unsigned *ticket, const double *__restrict__ z = nullptr) {
   if (S->status) return;
   constexpr int U = 2, MS = 8;  // nodes per thread, slots loaded ahead per node
+  const double bt = DIR ? S->beta : 0.0;
   double v[1] = {0.0};
   for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < m.npoin;
        base += (long long)gridDim.x * blockDim.x * U) {
@@ -387,18 +404,22 @@ k_cg_q(MeshDev m, const double *__restrict__ slots, const double *__restrict__ p
       const long long n = base + (long long)u * blockDim.x;
       b[u] = en[u] = 0;
       pn[u] = 0.0;
-      if (n < m.npoin) { b[u] = m.slot_ptr[n]; en[u] = m.slot_ptr[n + 1]; pn[u] = p[n]; }
+      if (n < m.npoin) {
+        b[u] = m.slot_ptr[n]; en[u] = m.slot_ptr[n + 1]; pn[u] = p[n];
+        if (DIR) pn[u] = z[n] + bt * pn[u];
+      }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const long long n = base + (long long)u * blockDim.x;
       if (n >= m.npoin) continue;
+      if (DIR && b[u] != en[u]) p[n] = pn[u];
       double sum = 0.0, cmp = 0.0;
       for (int s0 = b[u]; s0 < en[u]; s0 += MS) {
         int id[MS];
         double y[MS];
 #pragma unroll
-        for (int k = 0; k < MS; ++k) id[k] = s0 + k < en[u] ? m.slot_idx[s0 + k] : -1;
+        for (int k = 0; k < MS; ++k) id[k] = s0 + k < en[u] ? (DIR ? s0 + k : m.slot_idx[s0 + k]) : -1;
 #pragma unroll
         for (int k = 0; k < MS; ++k) y[k] = id[k] >= 0 ? slots[id[k]] : 0.0;
 #pragma unroll
@@ -543,31 +564,6 @@ k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const float *__restr
     S->beta = (tot[0] - tot[1]) / S->rz;
     S->rz = tot[0];
     if (!isfinite(S->beta)) S->status = 3;
-  }
-}
-
-// p = z + beta p
-__global__ void __launch_bounds__(CG_THREADS)
-k_cg_dir(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ z, double *__restrict__ p,
-         const CgScal *S) {
-  if (S->status) return;
-  constexpr int U = CG_U;
-  const double bt = S->beta;
-  for (long long base = (long long)blockIdx.x * blockDim.x * U + threadIdx.x; base < npoin_w;
-       base += (long long)gridDim.x * blockDim.x * U) {
-    int id[U];
-    double zv[U], pv[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const long long t = base + (long long)u * blockDim.x;
-      id[u] = t < npoin_w ? lpoin_w[t] : -1;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (id[u] >= 0) { zv[u] = z[id[u]]; pv[u] = p[id[u]]; }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (id[u] >= 0) p[id[u]] = zv[u] + bt * pv[u];
   }
 }
 

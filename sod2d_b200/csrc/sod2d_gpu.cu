@@ -1445,17 +1445,18 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
     res = std::sqrt(h1) / bnorm;
     return 0;
   };
-  // one iteration, entirely on the device: q = A p, alpha, x/r update,
-  // z = M r, beta, p = z + beta p
+  // one iteration, entirely on the device: p = z + beta p, q = A p, alpha,
+  // x/r update, z = M r, beta
   auto iteration = [&]() {
     const MeshDev md = c->md();
     dispatch(c, [&](auto L) {
       using LL = decltype(L);
       constexpr int P = LL::P_;
-      k_lap_elem<P, LL::EPB, double><<<LL::grid(c->nelem), LL::TPB, 0, st>>>(md, G.p, (double *)c->slotsB,
-                                                                             &G.S->status);
-      k_cg_q<<<cg_blocks(c->npoin, 2), CG_THREADS, 0, st>>>(md, (const double *)c->slotsB, G.p, G.q, G.S, G.gpart,
-                                                            G.ticket);
+      // the search direction p = z + beta p is formed inside these two
+      k_lap_elem<P, LL::EPB, double, true><<<LL::grid(c->nelem), LL::TPB, 0, st>>>(
+          md, G.p, (double *)c->slotsB, &G.S->status, G.z0, &G.S->beta);
+      k_cg_q<true><<<cg_blocks(c->npoin, 2), CG_THREADS, 0, st>>>(md, (const double *)c->slotsB, G.p, G.q, G.S,
+                                                                  G.gpart, G.ticket, G.z0);
       if (kind == 0) {
         k_cg_update<true><<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.p, G.q, G.Minv, x, G.r, G.z0,
                                                                      G.S, G.hist, CG_HIST, G.gpart, G.ticket);
@@ -1470,7 +1471,6 @@ int sod_gpu_pressure_solve(sod_gpu_ctx *c, const double *b_in, double *x, const 
                                                                        NT.params, D::O_ALPHA, G.z0, G.S, G.gpart,
                                                                        G.ticket);
       }
-      k_cg_dir<<<cg_blocks(nw, CG_U), CG_THREADS, 0, st>>>(nw, c->lpoin_w, G.z0, G.p, G.S);
       return 0;
     });
   };
