@@ -463,24 +463,30 @@ k_patch_bwd_elem(long long nelem, const int *__restrict__ pt, const double *__re
 // dB[k][j] = sum_e Y[e][k] W[e][j] + SA[e][k] X[e][j]; block b sums the
 // contiguous element range [b E / nb, (b+1) E / nb) in element order and
 // writes its partial to part[b * stride + O_B + k NP + j] (deterministic).
+// Each thread owns a tile of 4 modes x JB slots, so an element's row values
+// are loaded once per tile instead of once per entry.
 template <int P>
 __global__ void __launch_bounds__(256)
 k_patch_dB(long long nelem, const float *__restrict__ X, const float *__restrict__ W, const float *__restrict__ Y,
            const float *__restrict__ SA, float *__restrict__ part, long long stride) {
   using D = NetDims<P>;
-  constexpr int NP = D::NP, K = NET_K, CH = 8, ENT = (K * NP + 255) / 256;
-  __shared__ __align__(16) float Xs[CH][NP], Ws[CH][NP], Ys[CH][K], Ss[CH][K];
+  constexpr int NP = D::NP, K = NET_K, CH = 8, JB = (NP + 31) / 32, NPJ = 32 * JB;
+  static_assert(K == 32, "8 blocks of 4 modes");
+  __shared__ __align__(16) float Xs[CH][NPJ], Ws[CH][NPJ], Ys[CH][K], Ss[CH][K];
   const long long lo = nelem * blockIdx.x / gridDim.x, hi = nelem * (blockIdx.x + 1) / gridDim.x;
-  float acc[ENT];
+  const int k0 = 4 * (threadIdx.x / 32), j0 = JB * (threadIdx.x % 32);
+  float acc[4][JB];
 #pragma unroll
-  for (int q = 0; q < ENT; ++q) acc[q] = 0.f;
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < JB; ++b) acc[a][b] = 0.f;
   for (long long c0 = lo; c0 < hi; c0 += CH) {
     const int nc = (int)((hi - c0) < CH ? (hi - c0) : CH);
     __syncthreads();
-    for (int i = threadIdx.x; i < nc * NP; i += blockDim.x) {
-      const int el = i / NP, j = i % NP;
-      Xs[el][j] = X[(c0 + el) * NP + j];
-      Ws[el][j] = W[(c0 + el) * NP + j];
+    for (int i = threadIdx.x; i < nc * NPJ; i += blockDim.x) {
+      const int el = i / NPJ, j = i % NPJ;
+      Xs[el][j] = j < NP ? X[(c0 + el) * NP + j] : 0.f;
+      Ws[el][j] = j < NP ? W[(c0 + el) * NP + j] : 0.f;
     }
     for (int i = threadIdx.x; i < nc * K; i += blockDim.x) {
       const int el = i / K, k = i % K;
@@ -488,80 +494,118 @@ k_patch_dB(long long nelem, const float *__restrict__ X, const float *__restrict
       Ss[el][k] = SA[(c0 + el) * K + k];
     }
     __syncthreads();
+    for (int el = 0; el < nc; ++el) {
+      const float4 y4 = *reinterpret_cast<const float4 *>(&Ys[el][k0]);
+      const float4 s4 = *reinterpret_cast<const float4 *>(&Ss[el][k0]);
+      const float yv[4] = {y4.x, y4.y, y4.z, y4.w}, sv[4] = {s4.x, s4.y, s4.z, s4.w};
+      float wv[JB], xv[JB];
 #pragma unroll
-    for (int q = 0; q < ENT; ++q) {
-      const int idx = threadIdx.x + 256 * q;
-      if (idx < K * NP) {
-        const int k = idx / NP, j = idx % NP;
-        float s = acc[q];
-        for (int el = 0; el < nc; ++el) s = fmaf(Ys[el][k], Ws[el][j], fmaf(Ss[el][k], Xs[el][j], s));
-        acc[q] = s;
-      }
+      for (int b = 0; b < JB; ++b) { wv[b] = Ws[el][j0 + b]; xv[b] = Xs[el][j0 + b]; }
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < JB; ++b) acc[a][b] = fmaf(yv[a], wv[b], fmaf(sv[a], xv[b], acc[a][b]));
     }
   }
 #pragma unroll
-  for (int q = 0; q < ENT; ++q) {
-    const int idx = threadIdx.x + 256 * q;
-    if (idx < K * NP) part[blockIdx.x * stride + D::O_B + idx] = acc[q];
-  }
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < JB; ++b)
+      if (j0 + b < NP) part[blockIdx.x * stride + D::O_B + (k0 + a) * NP + j0 + b] = acc[a][b];
 }
 
 // Gradient of the gain MLP from dS = dL/ds; block b covers the same element
-// range as k_patch_dB, each warp accumulates its elements in a shared-memory
-// slice, the block sums the slices in warp order into part (deterministic).
+// range as k_patch_dB.  The weights are staged in shared memory (W2 and W3
+// also transposed, so the backward matrix-vector products read rows lane by
+// lane); each lane accumulates its column of every weight gradient in
+// registers over its warp's elements, and the block adds the warps'
+// gradients in warp order into part (deterministic).
 template <int P>
 __global__ void __launch_bounds__(256)
 k_mlp_bwd(long long nelem, const float *__restrict__ feat, const float *__restrict__ prm,
           const float *__restrict__ dS, float *__restrict__ part, long long stride) {
   using D = NetDims<P>;
-  constexpr int H = NET_H, K = NET_K, NM = D::NMLP;
-  constexpr int R_W1T = 0, R_B1 = R_W1T + NET_F * H, R_W2T = R_B1 + H, R_B2 = R_W2T + H * H, R_W3T = R_B2 + H,
+  constexpr int H = NET_H, K = NET_K, F = NET_F, NM = D::NMLP;
+  static_assert(H == 32 && K == 32, "one lane per hidden unit and per mode");
+  constexpr int R_W1T = 0, R_B1 = R_W1T + F * H, R_W2T = R_B1 + H, R_B2 = R_W2T + H * H, R_W3T = R_B2 + H,
                 R_B3 = R_W3T + H * K;
-  extern __shared__ __align__(16) float smem[];
+  __shared__ float sW1T[F * H], sb1[H], sW2T[H * H], sW2[H * H], sb2[H], sW3T[H * K], sW3[K * H], sb3[K];
+  __shared__ float acc[NM];
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarps = blockDim.x / 32;
-  float *Gw = smem + warp * NM;
-  for (int i = threadIdx.x; i < nwarps * NM; i += blockDim.x) smem[i] = 0.f;
+  for (int i = threadIdx.x; i < H * H; i += blockDim.x) {
+    const int r = i / H, q = i % H;
+    sW2T[i] = prm[D::O_W2T + i];
+    sW3T[i] = prm[D::O_W3T + i];
+    sW2[q * H + r] = prm[D::O_W2T + i];  // sW2[j][l] = W2T[l][j]
+    sW3[q * H + r] = prm[D::O_W3T + i];  // sW3[k][l] = W3T[l][k]
+  }
+  for (int i = threadIdx.x; i < F * H; i += blockDim.x) sW1T[i] = prm[D::O_W1T + i];
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    sb1[i] = prm[D::O_B1 + i];
+    sb2[i] = prm[D::O_B2 + i];
+    sb3[i] = prm[D::O_B3 + i];
+  }
+  for (int i = threadIdx.x; i < NM; i += blockDim.x) acc[i] = 0.f;
   __syncthreads();
+  float g3[H], g2[H], g1[F], gb3 = 0.f, gb2 = 0.f, gb1 = 0.f;
+#pragma unroll
+  for (int i = 0; i < H; ++i) { g3[i] = 0.f; g2[i] = 0.f; }
+#pragma unroll
+  for (int q = 0; q < F; ++q) g1[q] = 0.f;
   const long long lo = nelem * blockIdx.x / gridDim.x, hi = nelem * (blockIdx.x + 1) / gridDim.x;
-  const float *W2T = prm + D::O_W2T, *W3T = prm + D::O_W3T;
   for (long long e = lo + warp; e < hi; e += nwarps) {
-    float f[NET_F];
+    float f[F];
 #pragma unroll
-    for (int q = 0; q < NET_F; ++q) f[q] = feat[e * NET_F + q];
-    float a = prm[D::O_B1 + lane];
+    for (int q = 0; q < F; ++q) f[q] = feat[e * F + q];
+    float a = sb1[lane];
 #pragma unroll
-    for (int q = 0; q < NET_F; ++q) a = fmaf(prm[D::O_W1T + q * H + lane], f[q], a);
+    for (int q = 0; q < F; ++q) a = fmaf(sW1T[q * H + lane], f[q], a);
     const float h1 = tanhf(a);
-    a = prm[D::O_B2 + lane];
-    for (int i = 0; i < H; ++i) a = fmaf(W2T[i * H + lane], __shfl_sync(0xffffffffu, h1, i), a);
+    a = sb2[lane];
+#pragma unroll
+    for (int i = 0; i < H; ++i) a = fmaf(sW2T[i * H + lane], __shfl_sync(0xffffffffu, h1, i), a);
     const float h2 = tanhf(a);
-    a = prm[D::O_B3 + lane];
-    for (int i = 0; i < H; ++i) a = fmaf(W3T[i * K + lane], __shfl_sync(0xffffffffu, h2, i), a);
+    a = sb3[lane];
+#pragma unroll
+    for (int i = 0; i < H; ++i) a = fmaf(sW3T[i * K + lane], __shfl_sync(0xffffffffu, h2, i), a);
     const float dO = dS[e * K + lane] * sigmoidf(a);  // lane = mode
     // layer 3
-    Gw[R_B3 + lane] += dO;
-    for (int i = 0; i < H; ++i) Gw[R_W3T + i * K + lane] += __shfl_sync(0xffffffffu, h2, i) * dO;
-    float dh2 = 0.f;  // lane = hidden unit i
-    for (int k = 0; k < K; ++k) dh2 = fmaf(W3T[lane * K + k], __shfl_sync(0xffffffffu, dO, k), dh2);
+    gb3 += dO;
+#pragma unroll
+    for (int i = 0; i < H; ++i) g3[i] += __shfl_sync(0xffffffffu, h2, i) * dO;
+    float dh2 = 0.f;  // lane = hidden unit
+#pragma unroll
+    for (int k = 0; k < K; ++k) dh2 = fmaf(sW3[k * H + lane], __shfl_sync(0xffffffffu, dO, k), dh2);
     const float dz2 = dh2 * (1.f - h2 * h2);
     // layer 2
-    Gw[R_B2 + lane] += dz2;
-    for (int i = 0; i < H; ++i) Gw[R_W2T + i * H + lane] += __shfl_sync(0xffffffffu, h1, i) * dz2;
+    gb2 += dz2;
+#pragma unroll
+    for (int i = 0; i < H; ++i) g2[i] += __shfl_sync(0xffffffffu, h1, i) * dz2;
     float dh1 = 0.f;
-    for (int j = 0; j < H; ++j) dh1 = fmaf(W2T[lane * H + j], __shfl_sync(0xffffffffu, dz2, j), dh1);
+#pragma unroll
+    for (int j = 0; j < H; ++j) dh1 = fmaf(sW2[j * H + lane], __shfl_sync(0xffffffffu, dz2, j), dh1);
     const float dz1 = dh1 * (1.f - h1 * h1);
     // layer 1
-    Gw[R_B1 + lane] += dz1;
+    gb1 += dz1;
 #pragma unroll
-    for (int q = 0; q < NET_F; ++q) Gw[R_W1T + q * H + lane] += f[q] * dz1;
-    __syncwarp();
+    for (int q = 0; q < F; ++q) g1[q] += f[q] * dz1;
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i < NM; i += blockDim.x) {
-    float s = 0.f;
-    for (int w = 0; w < nwarps; ++w) s += smem[w * NM + i];
-    part[blockIdx.x * stride + D::O_W1T + i] = s;
+  for (int w = 0; w < nwarps; ++w) {
+    if (warp == w) {
+      acc[R_B3 + lane] += gb3;
+      acc[R_B2 + lane] += gb2;
+      acc[R_B1 + lane] += gb1;
+#pragma unroll
+      for (int i = 0; i < H; ++i) {
+        acc[R_W3T + i * K + lane] += g3[i];
+        acc[R_W2T + i * H + lane] += g2[i];
+      }
+#pragma unroll
+      for (int q = 0; q < F; ++q) acc[R_W1T + q * H + lane] += g1[q];
+    }
+    __syncthreads();
   }
+  for (int i = threadIdx.x; i < NM; i += blockDim.x) part[blockIdx.x * stride + D::O_W1T + i] = acc[i];
 }
 
 // dL/dalpha partial: exp(alpha) sum over the block's working nodes of

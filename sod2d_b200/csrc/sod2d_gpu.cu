@@ -2336,7 +2336,7 @@ void net_backward(sod_gpu_ctx *c, const double *r, const double *g, float *part)
     k_patch_bwd_elem<P><<<4 * 148, 256, D::bwd_smem(8), c->stream>>>(c->nelem, NT.pt, r, g, NT.Dh, NT.params,
                                                                      NT.gains, NT.X, NT.W, NT.Y, NT.SA, NT.dS);
     k_patch_dB<P><<<NT.nblk_bwd, 256, 0, c->stream>>>(c->nelem, NT.X, NT.W, NT.Y, NT.SA, part, stride);
-    k_mlp_bwd<P><<<NT.nblk_bwd, 256, (size_t)8 * D::NMLP * 4, c->stream>>>(c->nelem, NT.feat, NT.params, NT.dS,
+    k_mlp_bwd<P><<<NT.nblk_bwd, 256, 0, c->stream>>>(c->nelem, NT.feat, NT.params, NT.dS,
                                                                            part, stride);
     k_alpha_part<<<NT.nblk_bwd, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, r, g, NT.Dh, NT.params, D::O_ALPHA,
                                                      part, stride);
@@ -2485,14 +2485,12 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
       using D = NetDims<3>;
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
-      CUDA_TRY(cudaFuncSetAttribute(k_mlp_bwd<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * D::NMLP * 4));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)TcDims<3>::smem()));
     } else {
       using D = NetDims<4>;
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
-      CUDA_TRY(cudaFuncSetAttribute(k_mlp_bwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 8 * D::NMLP * 4));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)TcDims<4>::smem()));
     }
