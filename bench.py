@@ -41,9 +41,9 @@ sys.path.insert(0, str(ROOT))
 
 B_PER_NODE_STAGE = 402.0
 # DRAM bytes (read + write) of one RHS evaluation per working node, from one
-# ncu capture of the four RHS kernels on the 32^3 workload (548,663,296 B for
-# 884,736 working nodes), scaled by the working nodes of the benchmarked mesh.
-DRAM_B_PER_NODE_STAGE = 548663296 / 884736
+# ncu capture of the four RHS kernels on the 64^3 workload itself
+# (5,558,146,304 B for 7,077,888 working nodes).
+DRAM_B_PER_NODE_STAGE = 5558146304 / 7077888
 NELEM_1D = 64
 PORDER = 3
 
@@ -219,8 +219,8 @@ def run_reference(args, rank, world):
     return 0
 
 
-def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, train_steps=300, lr=1e-3, capacity=256,
-                 self_steps=16, ft_steps=200, ft_lr=5e-4, ft_batch=8):
+def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=None, train_steps=300, lr=1e-3, capacity=256,
+                 self_steps=16, ft_steps=200, ft_lr=5e-4, ft_batch=8, extrap_arm=True):
     """Pressure-Poisson solve to a 1e-8 FP64-certified relative residual on
     the incompressible Taylor-Green vortex (periodic cube nelem1d^3 HEX64,
     Re=1600): Jacobi-preconditioned flexible CG from the previous pressure
@@ -237,10 +237,14 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     the network is fine-tuned on those (`ft_steps` Adam steps) before the
     rest.  Training and fine-tuning time is reported apart from the solves,
     and `speedup_wall_amortized` charges it, with the extra solve time of
-    the harvesting steps, to the learned path."""
+    the harvesting steps, to the learned path.  `extrap_arm` False leaves out
+    the Jacobi trajectory from the extrapolated guess (large meshes, where
+    every arm costs minutes)."""
     import ctypes as C
     import torch
     from sod2d_b200 import gpu, host
+    if dt is None:  # 0.01 on the 32^3 mesh, the same convective CFL on finer meshes
+        dt = 0.01 * 32 / nelem1d
     m = host.periodic_cube(PORDER, nelem1d)
     N = m.npoin
     x, y, z = (m.coord[i * N:(i + 1) * N].astype(np.float64) for i in range(3))
@@ -250,7 +254,7 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     # ctxs[0]: learned trajectory (harvests during the Jacobi steps);
     # ctxs[1]: Jacobi from the previous pressure (the reference's guess);
     # ctxs[2]: Jacobi from the learned path's guess 2 p^n - p^(n-1)
-    ctxs = [gpu.Context(m, gpu.default_phys()) for _ in range(3)]
+    ctxs = [gpu.Context(m, gpu.default_phys()) for _ in range(3 if extrap_arm else 2)]
     for c in ctxs:
         c.call("sod_gpu_incomp_init", gpu.dptr(u0), nu)
     ctxs[0].call("sod_gpu_precond_init", 2024, capacity)
@@ -271,8 +275,10 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
     div = torch.zeros(N, device="cuda")
     w = torch.from_numpy((m.lpoin_w - 1).astype(np.int64)).cuda()
     ft_s, ft_loss, ft_pairs = 0.0, C.c_float(), 0
-    for i, (name, kind) in enumerate((("jacobi", 0), ("jacobi_extrapolated_guess", 3), ("learned", 1))):
-        c = {0: ctxs[1], 3: ctxs[2], 1: ctxs[0]}[kind]
+    peak_used = [0]  # device memory in use (all contexts and torch), sampled every 50 steps
+    arms = (("jacobi", 0), ("jacobi_extrapolated_guess", 3), ("learned", 1))
+    for i, (name, kind) in enumerate(a for a in arms if extrap_arm or a[1] != 3):
+        c = {0: ctxs[1], 3: ctxs[-1], 1: ctxs[0]}[kind]
         it, ms, rmax, fb, dv, vits, step_ms = [], [], 0.0, 0, [], [], []
         vit = C.c_int()
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -300,17 +306,23 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
             dv.append(float(div[w].double().norm()))
             c.call("sod_gpu_incomp_veloc_stats", C.byref(vit), None)
             vits.append(vit.value)
+            if k % 50 == 0:
+                free, total = torch.cuda.mem_get_info()
+                peak_used[0] = max(peak_used[0], int(total - free))
         res[name] = {"mean_iterations": round(float(np.mean(it)), 1), "mean_solve_ms": round(float(np.mean(ms)), 3),
                      "mean_velocity_cg_iterations": round(float(np.mean(vits)), 2),
                      "mean_step_ms": round(float(np.mean(step_ms)), 3),
                      "max_true_residual": rmax, "fallbacks": fb, "mean_div_u_l2": float(np.mean(dv)),
                      "mean_solve_ms_first_100": round(float(np.mean(ms[:100])), 3),
                      "total_solve_s": round(float(np.sum(ms)) / 1e3, 3),
-                     "iterations_every_50_steps": it[::50]}
+                     "iterations_every_50_steps": it[::50],
+                     # the rest of the step (convection, diffusion, velocity solve, BDF/EXT, div/grad)
+                     "step_without_pressure_Mnodes_per_s": round(m.npoin_w / max(1e-9, float(np.mean(step_ms)) -
+                                                                                 float(np.mean(ms))) / 1e3, 1)}
     dev_bytes = [c.device_bytes for c in ctxs]
     for c in ctxs:
         c.close()
-    return {"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt}, "
+    return {"workload": f"incompressible TGV, periodic cube {nelem1d}^3 HEX64 ({N} nodes), Re=1600, dt={dt:.6g}, "
                         f"BDF3/EXT3-step pressure systems, FP64-certified tol 1e-8",
             "harvest_steps": harvest_steps, "compare_steps": compare_steps, "harvest_capacity": capacity,
             "train_steps": train_steps, "train_batch": 16, "train_lr": lr, "train_seconds": round(train_s, 2),
@@ -318,10 +330,10 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
             "self_harvest_steps": self_steps, "self_harvest_pairs": ft_pairs, "finetune_steps": ft_steps,
             "finetune_batch": ft_batch, "finetune_lr": ft_lr, "finetune_seconds": round(ft_s, 2),
             "finetune_loss": round(float(ft_loss.value), 4), "jacobi": res["jacobi"],
-            "jacobi_extrapolated_guess": res["jacobi_extrapolated_guess"], "learned": res["learned"],
+            "jacobi_extrapolated_guess": res.get("jacobi_extrapolated_guess"), "learned": res["learned"],
             "speedup_wall": round(res["jacobi"]["mean_solve_ms"] / res["learned"]["mean_solve_ms"], 3),
-            "speedup_wall_vs_jacobi_same_guess": round(res["jacobi_extrapolated_guess"]["mean_solve_ms"] /
-                                                       res["learned"]["mean_solve_ms"], 3),
+            "speedup_wall_vs_jacobi_same_guess": (round(res["jacobi_extrapolated_guess"]["mean_solve_ms"] /
+                                                        res["learned"]["mean_solve_ms"], 3) if extrap_arm else None),
             "harvest_overhead_s": round((harvest_ms[0] - harvest_ms[1]) / 1e3, 3),
             "speedup_wall_amortized": round(res["jacobi"]["total_solve_s"] /
                                             (res["learned"]["total_solve_s"] + train_s + ft_s +
@@ -333,7 +345,8 @@ def pressure_leg(nelem1d=32, harvest_steps=200, compare_steps=800, dt=0.01, trai
                                                   res["learned"]["mean_solve_ms_first_100"], 3),
             "device_bytes_jacobi_ctx": dev_bytes[1], "device_bytes_learned_ctx": dev_bytes[0],
             "harvest_seconds": round(harvest_ms[0] / 1e3, 3),
-            "torch_peak_bytes": int(torch.cuda.max_memory_allocated())}
+            "torch_peak_bytes": int(torch.cuda.max_memory_allocated()),
+            "device_used_bytes_peak": peak_used[0]}
 
 
 def time_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3):
@@ -372,6 +385,8 @@ def imex_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3, Ma=1.25, cfl=0
     import ctypes as C
     import torch
     from sod2d_b200 import gpu, host
+    if dt is None:  # 0.01 on the 32^3 mesh, the same convective CFL on finer meshes
+        dt = 0.01 * 32 / nelem1d
     m = host.periodic_cube(PORDER, nelem1d)
     ic = host.tgv_comp_init(m, Ma=Ma)
     sv = gpu.CompSolver(m, ic, stages=stages, fp64_state=False, cfl_conv=cfl, cfl_diff=1000.5, imex=True)
@@ -525,6 +540,8 @@ def main():
     ap.add_argument("--p-self", type=int, default=16,
                     help="learned steps that harvest from their own solves before fine-tuning (0: none)")
     ap.add_argument("--p-finetune", type=int, default=200, help="Adam steps of the fine-tuning")
+    ap.add_argument("--p-no-extrap", action="store_true",
+                    help="leave out the Jacobi arm from the extrapolated guess (large meshes)")
     ap.add_argument("--precision-study", action="store_true",
                     help="run only the FP32/FP64 precision study against the FP64 oracle (prints its JSON object)")
     ap.add_argument("--ps-nelem1d", type=int, default=16)
@@ -534,7 +551,8 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     pkw = dict(nelem1d=args.p_nelem1d, harvest_steps=args.p_harvest, compare_steps=args.p_compare,
-               train_steps=args.p_train, capacity=args.p_capacity, self_steps=args.p_self, ft_steps=args.p_finetune)
+               train_steps=args.p_train, capacity=args.p_capacity, self_steps=args.p_self, ft_steps=args.p_finetune,
+               extrap_arm=not args.p_no_extrap)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -705,7 +723,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": int(round(DRAM_B_PER_NODE_STAGE * m.npoin_w)),
-                     "traffic_source": "ncu dram__bytes_read+write of the 4 RHS kernels at 32^3, scaled by working nodes",
+                     "traffic_source": "ncu dram__bytes_read+write of the 4 RHS kernels at 64^3 (per working node, times "
+                                       "this mesh's working nodes)",
                      "peak_source": f"{peak_kind} copy bandwidth (MEASURED_PEAKS.json hbm_gbs)",
                      "unit_of_work": "one fused RHS evaluation (4 launches): 402 B x working nodes"},
         "e2e": {"value": round(e2e_val, 2), "unit": "Mnode-stages/s", "h2d_bytes_per_step": h2d,

@@ -3,7 +3,10 @@
 * ``_lib/libsod2d_host.so``  -- host-side set-up (mesh, GLL tables, Jacobians);
   plain C++, no GPU needed.
 * ``_lib/libsod2d_gpu.so``   -- the sm_100a CUDA kernels behind the C-ABI of
-  ``include/sod2d_gpu.h``.
+  ``include/sod2d_gpu.h``, linked from one object per translation unit
+  (``sod2d_gpu.cu`` context and compressible RHS, ``comp_step.cu`` time
+  integrators, ``incomp.cu`` incompressible path, ``precond.cu`` learned
+  preconditioner, ``noalloc_analysis.cu``).
 
 Both land inside the package directory so they travel with the source tree.
 """
@@ -18,6 +21,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
+OBJDIR = PKG / "_build"  # object files (not committed)
 INCLUDE = ROOT / "include"
 
 # The image exports CXX=/opt/gcc/bin/g++, which lacks libgomp: use the system
@@ -27,7 +31,7 @@ NVCC = os.environ.get("SOD2D_NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 HOST_SRCS = ["host_setup.cpp"]
-GPU_SRCS = ["sod2d_gpu.cu", "noalloc_analysis.cu"]
+GPU_SRCS = ["sod2d_gpu.cu", "comp_step.cu", "incomp.cu", "precond.cu", "noalloc_analysis.cu"]
 
 
 def _stale(target: Path, deps) -> bool:
@@ -53,14 +57,28 @@ def build_host(force: bool = False) -> Path:
 
 
 def build_gpu(force: bool = False) -> Path:
+    """Each translation unit is compiled on its own (in parallel, and only
+    when it or a header changed), then linked into one shared library."""
+    from concurrent.futures import ThreadPoolExecutor
     LIBDIR.mkdir(exist_ok=True)
+    OBJDIR.mkdir(exist_ok=True)
     out = LIBDIR / "libsod2d_gpu.so"
-    srcs = [CSRC / s for s in GPU_SRCS]
-    deps = srcs + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "sod2d_gpu.h"]
-    if force or _stale(out, deps):
-        _run([NVCC, ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-shared", f"-I{INCLUDE}", f"-I{CSRC}", "--expt-relaxed-constexpr",
-              f"-ccbin={HOST_CXX}", *map(str, srcs), "-o", str(out)])
+    headers = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + [INCLUDE / "sod2d_gpu.h"]
+    flags = [ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INCLUDE}", f"-I{CSRC}",
+             "--expt-relaxed-constexpr", f"-ccbin={HOST_CXX}"]
+    objs = []
+    jobs = []
+    for name in GPU_SRCS:
+        src = CSRC / name
+        obj = OBJDIR / (src.stem + ".o")
+        objs.append(obj)
+        if force or _stale(obj, [src] + headers):
+            jobs.append([NVCC, *flags, "-c", str(src), "-o", str(obj)])
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+            list(ex.map(_run, jobs))
+    if force or jobs or _stale(out, objs):
+        _run([NVCC, ARCH, "-shared", f"-ccbin={HOST_CXX}", *map(str, objs), "-o", str(out)])
     return out
 
 

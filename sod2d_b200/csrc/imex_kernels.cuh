@@ -20,7 +20,7 @@ struct ImexCoef {
 // source, wall model or buoyancy):
 //   U2 = -dt R_stab - sum_{j<is} (dt ae(is,j) R_j + dt ai(is,j) D_j) + U1 Ml
 // R, D: stage-major five-variable blocks; stab, lvl1: five-variable blocks.
-__global__ void k_imex_comb(long long npoin, int is, ImexCoef k, float dt, const float *__restrict__ Ml,
+static __global__ void k_imex_comb(long long npoin, int is, ImexCoef k, float dt, const float *__restrict__ Ml,
                             const float *__restrict__ R, const float *__restrict__ D, const float *__restrict__ stab,
                             const float *__restrict__ lvl1, float *__restrict__ rho2, float *__restrict__ E2,
                             float *__restrict__ q2) {
@@ -42,7 +42,7 @@ __global__ void k_imex_comb(long long npoin, int is, ImexCoef k, float dt, const
 }
 
 // h = gamma/(gamma-1) p / rho over the working nodes (time_integ_imex.f90:433)
-__global__ void k_aux_h(int npoin_w, const int *__restrict__ lpoin_w, float g_gm1, const float *__restrict__ rho,
+static __global__ void k_aux_h(int npoin_w, const int *__restrict__ lpoin_w, float g_gm1, const float *__restrict__ rho,
                         const float *__restrict__ pr, float *__restrict__ h) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
@@ -53,7 +53,7 @@ __global__ void k_aux_h(int npoin_w, const int *__restrict__ lpoin_w, float g_gm
 // Velocity and temperature of the CG argument v over the iterate's density
 // (mod_solver_imex.f90:97-107, 160-167, 310-320): u = v_mom / x_mass,
 // T = x_mass (gamma-1) (v_E / x_mass - |u|^2/2) / (x_mass Rgas).
-__global__ void k_imex_prim(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, float gm1, float Rgas,
+static __global__ void k_imex_prim(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, float gm1, float Rgas,
                             const float *__restrict__ x, const float *__restrict__ v, float *__restrict__ au,
                             float *__restrict__ aT) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -72,7 +72,7 @@ __global__ void k_imex_prim(int npoin_w, long long npoin, const int *__restrict_
 }
 
 // qn = v Ml + qn fact dt over the working nodes, five variables
-__global__ void k_imex_op(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ Ml,
+static __global__ void k_imex_op(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ Ml,
                           const float *__restrict__ v, float fact, float dt, float *__restrict__ qn) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
@@ -89,7 +89,7 @@ __global__ void k_imex_op(int npoin_w, long long npoin, const int *__restrict__ 
 //   mode 0: r = b - qn; z = r / M; p = z
 //   mode 1: x += alpha p; r -= alpha qn; z1 = z; z = r / M
 //   mode 2: p = z + beta p
-__global__ void k_imex_vec(int mode, int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
+static __global__ void k_imex_vec(int mode, int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
                            const float *__restrict__ Ml, float dt, float alpha, float beta,
                            const float *__restrict__ b, float *__restrict__ x, float *__restrict__ r,
                            float *__restrict__ p, const float *__restrict__ qn, float *__restrict__ z,
@@ -120,7 +120,7 @@ __global__ void k_imex_vec(int mode, int npoin_w, long long npoin, const int *__
 }
 
 // (rho, E, q) = x over the working nodes (mod_solver_imex.f90:331-338)
-__global__ void k_imex_out(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ x,
+static __global__ void k_imex_out(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ x,
                            float *__restrict__ rho, float *__restrict__ E, float *__restrict__ q) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;

@@ -221,7 +221,7 @@ struct DotArgs {
 };
 
 // Single-block sum of DOT_BLOCKS partials per value, in a fixed order.
-__global__ void k_dot_final(int nd, const double *__restrict__ part, double *__restrict__ out) {
+static __global__ void k_dot_final(int nd, const double *__restrict__ part, double *__restrict__ out) {
   __shared__ double sh[1024];
   for (int d = 0; d < nd; ++d) {
     double s = 0.0;
@@ -520,7 +520,7 @@ k_cg_update(int npoin_w, const int *__restrict__ lpoin_w, const double *__restri
 // the node's contributions, stored contiguously from pptr[n]) (as
 // k_patch_gather_perm), with the partials r.z and r.z_old; the last block
 // sets beta and rz.
-__global__ void __launch_bounds__(CG_THREADS)
+static __global__ void __launch_bounds__(CG_THREADS)
 k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const float *__restrict__ ctr,
              const double *__restrict__ r, const double *__restrict__ Dh, const float *__restrict__ prm, int o_alpha,
              double *__restrict__ z, CgScal *S, double *__restrict__ part, unsigned *ticket) {
@@ -568,7 +568,7 @@ k_cg_patch_z(long long npoin, const int *__restrict__ pptr, const float *__restr
 }
 
 // harvest snapshot of the iterate and residual (skipped once stopped)
-__global__ void k_cg_snapshot(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ x,
+static __global__ void k_cg_snapshot(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ x,
                               const double *__restrict__ r, double *__restrict__ xs, float *__restrict__ rs,
                               const CgScal *S) {
   if (S->status) return;

@@ -254,7 +254,7 @@ __device__ __forceinline__ void mma_tf32(float (&c)[4], uint32_t a0, uint32_t a1
 }
 
 // uf = (float)(D^-1/2 r) over the working nodes
-__global__ void k_scale_f32(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
+static __global__ void k_scale_f32(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
                             const double *__restrict__ Dh, float *__restrict__ uf) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
@@ -389,7 +389,7 @@ k_patch_apply_tc(long long nelem, const int *__restrict__ pt, const int *__restr
 
 // z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of the node's
 // contributions, stored contiguously from pptr[n]), FP64.
-__global__ void k_patch_gather_perm(long long npoin, const int *__restrict__ pptr, const float *__restrict__ ctr,
+static __global__ void k_patch_gather_perm(long long npoin, const int *__restrict__ pptr, const float *__restrict__ ctr,
                                     const double *__restrict__ r, const double *__restrict__ Dh,
                                     const float *__restrict__ prm, int o_alpha, double *__restrict__ z) {
   const long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -404,7 +404,7 @@ __global__ void k_patch_gather_perm(long long npoin, const int *__restrict__ ppt
 
 // z(n) = D^-1/2(n) (exp(alpha) D^-1/2(n) r(n) + sum of the node's patch
 // slots), FP64, for nodes that own patch slots (the working nodes).
-__global__ void k_patch_gather(long long npoin, const int *__restrict__ pptr, const int *__restrict__ pslot,
+static __global__ void k_patch_gather(long long npoin, const int *__restrict__ pptr, const int *__restrict__ pslot,
                                const float *__restrict__ slots, const double *__restrict__ r,
                                const double *__restrict__ Dh, const float *__restrict__ prm, int o_alpha,
                                double *__restrict__ z) {
@@ -610,7 +610,7 @@ k_mlp_bwd(long long nelem, const float *__restrict__ feat, const float *__restri
 
 // dL/dalpha partial: exp(alpha) sum over the block's working nodes of
 // (D^-1/2 g)(D^-1/2 r), written to part[b * stride + o_alpha].
-__global__ void k_alpha_part(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
+static __global__ void k_alpha_part(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
                              const double *__restrict__ g, const double *__restrict__ Dh,
                              const float *__restrict__ prm, int o_alpha, float *__restrict__ part, long long stride) {
   __shared__ double sh[256];
@@ -631,7 +631,7 @@ __global__ void k_alpha_part(int npoin_w, const int *__restrict__ lpoin_w, const
 }
 
 // grad[i] = sum over blocks of part[b][i] (fixed order), then Adam.
-__global__ void k_adam(int nparam, int nblocks, const float *__restrict__ part, float *__restrict__ params,
+static __global__ void k_adam(int nparam, int nblocks, const float *__restrict__ part, float *__restrict__ params,
                        float *__restrict__ m1, float *__restrict__ m2, float lr, float b1, float b2, float eps,
                        float bc1, float bc2, float gscale, float *__restrict__ grad_out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -67,8 +67,7 @@ __device__ __forceinline__ void iso_grad(const float *__restrict__ f, int i, int
                                          const float (&Dk)[P + 1], float &g0, float &g1, float &g2) {
   constexpr int N1 = P + 1;
   g0 = 0.f; g1 = 0.f; g2 = 0.f;
-#if SOD_VEC_XI
-  if constexpr (P == 3) {
+  if constexpr (P == 3 && SOD_VEC_XI) {
     // the xi-line of a 4-node element row is one aligned 16-byte load
     const float4 v = *reinterpret_cast<const float4 *>(f + 4 * j + 16 * k);
     const float fx[4] = {v.x, v.y, v.z, v.w};
@@ -79,15 +78,14 @@ __device__ __forceinline__ void iso_grad(const float *__restrict__ f, int i, int
       g1 = fmaf(Dj[m], f[i + N1 * m + N1 * N1 * k], g1);
       g2 = fmaf(Dk[m], f[i + N1 * j + N1 * N1 * m], g2);
     }
-    return;
-  }
-#endif
+  } else {
 #pragma unroll
-  for (int s = 0; s < N1; ++s) {
-    const int m = ref_order<P>(s);
-    g0 = fmaf(Di[m], f[m + N1 * j + N1 * N1 * k], g0);
-    g1 = fmaf(Dj[m], f[i + N1 * m + N1 * N1 * k], g1);
-    g2 = fmaf(Dk[m], f[i + N1 * j + N1 * N1 * m], g2);
+    for (int s = 0; s < N1; ++s) {
+      const int m = ref_order<P>(s);
+      g0 = fmaf(Di[m], f[m + N1 * j + N1 * N1 * k], g0);
+      g1 = fmaf(Dj[m], f[i + N1 * m + N1 * N1 * k], g1);
+      g2 = fmaf(Dk[m], f[i + N1 * j + N1 * N1 * m], g2);
+    }
   }
 }
 
@@ -730,7 +728,7 @@ __global__ void k_gather(MeshDev m, const float *__restrict__ slots, float *__re
 // ---------------------------------------------------------------------
 // The 5 residuals from node-sorted pass-B slots into the reference's SoA
 // outputs (optionally accumulated onto them), x invMl.
-__global__ void k_gather_sorted_res5(MeshDev m, const float *__restrict__ slots, long long zoff, OutPtrs out_soa,
+static __global__ void k_gather_sorted_res5(MeshDev m, const float *__restrict__ slots, long long zoff, OutPtrs out_soa,
                                      int accumulate, int use_invMl) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= m.npoin) return;

@@ -41,7 +41,7 @@ __global__ void k_stage(int npoin_w, long long npoin, const int *__restrict__ lp
 }
 
 // ---- end-of-step EOS (time_integ_ls.f90:391-407) -----------------------
-__global__ void k_eos_end(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, float gm1, float gamma,
+static __global__ void k_eos_end(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, float gm1, float gamma,
                           float Rgas, const float *__restrict__ rho, const float *__restrict__ q,
                           const float *__restrict__ E, float *__restrict__ u, float *__restrict__ eint,
                           float *__restrict__ pr, float *__restrict__ csound, float *__restrict__ machno,
@@ -71,7 +71,7 @@ __global__ void k_eos_end(int npoin_w, long long npoin, const int *__restrict__ 
 // ---- thermo_entropy, mod_entropy_viscosity.f90:411-433 ----------------
 // eta1 <- eta2; eta2 <- rho/(g-1) log(max(p/p_inf, eps)/(rho/rho_inf)^g);
 // feta = u1 * eta1.
-__global__ void k_thermo_entropy(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, float gamma,
+static __global__ void k_thermo_entropy(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, float gamma,
                                  float p_inf, float rho_inf, const float *__restrict__ rho,
                                  const float *__restrict__ pr, const float *__restrict__ u1,
                                  float *__restrict__ eta1, float *__restrict__ eta2, float *__restrict__ feta) {
@@ -87,7 +87,7 @@ __global__ void k_thermo_entropy(int npoin_w, long long npoin, const int *__rest
 }
 
 // feta = u1 * eta1 at working nodes (first step, time_integ_ls.f90:274-281).
-__global__ void k_feta(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ u1,
+static __global__ void k_feta(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, const float *__restrict__ u1,
                        const float *__restrict__ eta1, float *__restrict__ feta) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
@@ -174,7 +174,7 @@ k_entropy_elem(MeshDev m, const float *__restrict__ feta, const float *__restric
 
 // Gather of the entropy pass: Reta (lumped: x invMl at working nodes),
 // divU (raw), curl / lelpn (working nodes).  Kahan-compensated, element order.
-__global__ void k_gather_entropy(MeshDev m, const float *__restrict__ slots, const int *__restrict__ lelpn,
+static __global__ void k_gather_entropy(MeshDev m, const float *__restrict__ slots, const int *__restrict__ lelpn,
                                  const int *__restrict__ is_work, float *__restrict__ Reta, float *__restrict__ divU,
                                  float *__restrict__ vort, int want_dc) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -203,7 +203,7 @@ __global__ void k_gather_entropy(MeshDev m, const float *__restrict__ slots, con
 }
 
 // auxReta = (1.5 R2 - 0.5 R1) + (eta2 - eta1)/dt; R1 <- R2 (time_integ_ls.f90:437-443)
-__global__ void k_aux_reta(int npoin_w, const int *__restrict__ lpoin_w, float dt, float *__restrict__ Reta1,
+static __global__ void k_aux_reta(int npoin_w, const int *__restrict__ lpoin_w, float dt, float *__restrict__ Reta1,
                            const float *__restrict__ Reta2, const float *__restrict__ eta1,
                            const float *__restrict__ eta2, float *__restrict__ aux) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -216,7 +216,7 @@ __global__ void k_aux_reta(int npoin_w, const int *__restrict__ lpoin_w, float d
 // Minimum of rho over working nodes (order-independent, deterministic).
 // grid of the node min / max reductions: 8 blocks of 256 per SM
 constexpr int MINMAX_BLOCKS = 148 * 8;
-__global__ void k_min_rho(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ rho,
+static __global__ void k_min_rho(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ rho,
                           unsigned int *__restrict__ out_bits) {
   float v = 100000.0f;
   // four strides per trip with every load issued first (min is order-free)
@@ -326,7 +326,7 @@ __global__ void k_ducros(MeshDev m, const float *__restrict__ u, const float *__
 // nodes, five fields (rho, E, q x/y/z): first stage U2 += (gam dt) R
 // (time_integ_ls.f90:325-329), later stages U2 = l1 U1 + li U2 + (gam dt) R
 // (:352-356), rounded as the reference (no contraction).
-__global__ void k_ls_stage_ref(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, int first, float l1,
+static __global__ void k_ls_stage_ref(int npoin_w, long long npoin, const int *__restrict__ lpoin_w, int first, float l1,
                                float li, float gam, float dt, const float *__restrict__ rho1,
                                const float *__restrict__ q1, const float *__restrict__ E1, float *__restrict__ rho2,
                                float *__restrict__ q2, float *__restrict__ E2, const float *__restrict__ Rmass,
@@ -349,7 +349,7 @@ __global__ void k_ls_stage_ref(int npoin_w, long long npoin, const int *__restri
 }
 
 // Sutherland viscosity at working nodes.
-__global__ void k_sutherland(int npoin_w, const int *__restrict__ lpoin_w, float mu_factor,
+static __global__ void k_sutherland(int npoin_w, const int *__restrict__ lpoin_w, float mu_factor,
                              const float *__restrict__ Tem, float *__restrict__ mu) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= npoin_w) return;
@@ -462,7 +462,7 @@ k_analysis_elem(MeshDev m, const float *__restrict__ rho, const float *__restric
 }
 
 // Deterministic FP64 sum of per-element partials: one block, fixed order.
-__global__ void k_sum_parts(long long nelem, const float *__restrict__ part, double *__restrict__ out3) {
+static __global__ void k_sum_parts(long long nelem, const float *__restrict__ part, double *__restrict__ out3) {
   __shared__ double sh[3][1024];
   const int t = threadIdx.x;
   double s[3] = {0.0, 0.0, 0.0};
@@ -479,7 +479,7 @@ __global__ void k_sum_parts(long long nelem, const float *__restrict__ part, dou
     for (int q = 0; q < 3; ++q) out3[q] = sh[q][0];
 }
 
-__global__ void k_max_mach(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ machno,
+static __global__ void k_max_mach(int npoin_w, const int *__restrict__ lpoin_w, const float *__restrict__ machno,
                            unsigned int *__restrict__ out_bits) {
   float v = 0.f;
   const int stride = gridDim.x * blockDim.x;

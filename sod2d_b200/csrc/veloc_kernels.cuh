@@ -12,7 +12,7 @@ namespace sod {
 
 // species_tau, src/lib_species/sources/elem_stab_species.f90:122-148:
 // tau_e = max over the element nodes of helem (c / p) |u|; warp per element.
-__global__ void k_species_tau(long long nelem, int N, const int *__restrict__ conn, const float *__restrict__ helem,
+static __global__ void k_species_tau(long long nelem, int N, const int *__restrict__ conn, const float *__restrict__ helem,
                               const float *__restrict__ u, long long npoin, float c_over_p, float *__restrict__ tau) {
   const long long e = (long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
   const int lane = threadIdx.x % 32;
@@ -85,7 +85,7 @@ k_tauv_elem(MeshDev m, const float *__restrict__ u, float *__restrict__ slots) {
 // Assembly of the projection slots (Kahan, element order) divided by the
 // lumped mass (lumped_solver_vect, mod_solver.f90:61-79), node-major
 // [npoin][8] (6 used); nodes without slots get 0.
-__global__ void k_gather_tauv(MeshDev m, const float *__restrict__ slots, const float *__restrict__ Ml,
+static __global__ void k_gather_tauv(MeshDev m, const float *__restrict__ slots, const float *__restrict__ Ml,
                               float *__restrict__ tauP) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= m.npoin) return;
@@ -114,7 +114,7 @@ __global__ void k_gather_tauv(MeshDev m, const float *__restrict__ slots, const 
 }
 
 // Reference layout GradX/GradY/GradZ (npoin,3) <-> node-major symmetric [p][8].
-__global__ void k_unpack_tauv(long long npoin, const float *__restrict__ tauP, float *__restrict__ GX,
+static __global__ void k_unpack_tauv(long long npoin, const float *__restrict__ tauP, float *__restrict__ GX,
                               float *__restrict__ GY, float *__restrict__ GZ) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoin) return;
@@ -123,7 +123,7 @@ __global__ void k_unpack_tauv(long long npoin, const float *__restrict__ tauP, f
   GY[p] = s[1]; GY[p + npoin] = s[3]; GY[p + 2 * npoin] = s[4];
   GZ[p] = s[2]; GZ[p + npoin] = s[4]; GZ[p + 2 * npoin] = s[5];
 }
-__global__ void k_pack_tauv(long long npoin, const float *__restrict__ GX, const float *__restrict__ GY,
+static __global__ void k_pack_tauv(long long npoin, const float *__restrict__ GX, const float *__restrict__ GY,
                             const float *__restrict__ GZ, float *__restrict__ tauP) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npoin) return;
@@ -200,7 +200,7 @@ k_diffv_elem(MeshDev m, const float *__restrict__ u, const float *__restrict__ m
 }
 
 // qn = v Ml + qn fact dt over working nodes, 3 components (npoin,3)
-__global__ void k_veloc_op(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
+static __global__ void k_veloc_op(int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
                            const float *__restrict__ Ml, const float *__restrict__ v, float fact, float dt,
                            float *__restrict__ qn) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -218,7 +218,7 @@ __global__ void k_veloc_op(int npoin_w, long long npoin, const int *__restrict__
 // mode 0: r = b - qn ; z = r / (Ml/dt) ; p = z
 // mode 1: x += alpha p ; r -= alpha q ; z1 = z ; z = r / (Ml/dt)
 // mode 2: p = z + beta p
-__global__ void k_veloc_vec(int mode, int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
+static __global__ void k_veloc_vec(int mode, int npoin_w, long long npoin, const int *__restrict__ lpoin_w,
                             const float *__restrict__ Ml, float dt, float alpha, float beta,
                             const float *__restrict__ b, float *__restrict__ x, float *__restrict__ r,
                             float *__restrict__ p, const float *__restrict__ q, float *__restrict__ z,
