@@ -79,12 +79,12 @@ struct sod_gpu_ctx {
   // learned preconditioner
   struct Net {
     bool ready = false, gains_ok = false;
-    int nparam = 0, nblk_bwd = 148, step = 0, NP = 0;
+    int nparam = 0, nblk_bwd = 0, step = 0, NP = 0;
     float *params = nullptr, *m1 = nullptr, *m2 = nullptr, *part = nullptr, *grad = nullptr;
     int *pt = nullptr, *pptr = nullptr, *pslot = nullptr;   // patch table [E][NP]; node -> patch-slot CSR
     int *pos = nullptr;                                      // CSR position of each patch slot [E][NP]
     float *feat = nullptr, *gains = nullptr;                  // [E][8], [E][32]
-    float *X = nullptr, *W = nullptr, *Y = nullptr, *SA = nullptr, *dS = nullptr;  // training scratch
+    float *dS = nullptr;  // training scratch: dL/ds per element and mode
     double *Dh = nullptr;                                     // D^-1/2
     float *uf = nullptr;                                      // (float) D^-1/2 r for tensor-core inference
     // harvested (r, e) pairs, FP32, reservoir-sampled, and e^T A e per pair

@@ -94,37 +94,32 @@ namespace {
 
 int ensure_train_scratch(sod_gpu_ctx *c) {
   auto &NT = c->net;
-  if (NT.X) return 0;
-  const size_t E = (size_t)c->nelem;
-  int rc;
-  if ((rc = c->alloc(&NT.X, E * NT.NP)) || (rc = c->alloc(&NT.W, E * NT.NP)) || (rc = c->alloc(&NT.Y, E * NET_K)) ||
-      (rc = c->alloc(&NT.SA, E * NET_K)) || (rc = c->alloc(&NT.dS, E * NET_K)))
-    return rc;
-  return 0;
+  if (NT.dS) return 0;
+  return c->alloc(&NT.dS, (size_t)c->nelem * NET_K);
 }
 
 // Parameter-gradient partials of g = dL/dz at the residual r into part
-// (nblk_bwd rows of nparam floats).
-void net_backward(sod_gpu_ctx *c, const double *r, const double *g, float *part) {
+// (nblk_bwd rows of nparam floats), or added to them (accumulate).
+void net_backward(sod_gpu_ctx *c, const double *r, const double *g, float *part, int accumulate) {
   auto &NT = c->net;
   const long long stride = NT.nparam;
   dispatch(c, [&](auto L) {
     using LL = decltype(L);
     constexpr int P = LL::P_;
     using D = NetDims<P>;
-    k_patch_bwd_elem<P><<<4 * 148, 256, D::bwd_smem(8), c->stream>>>(c->nelem, NT.pt, r, g, NT.Dh, NT.params,
-                                                                     NT.gains, NT.X, NT.W, NT.Y, NT.SA, NT.dS);
-    k_patch_dB<P><<<NT.nblk_bwd, 256, 0, c->stream>>>(c->nelem, NT.X, NT.W, NT.Y, NT.SA, part, stride);
-    k_mlp_bwd<P><<<NT.nblk_bwd, 256, 0, c->stream>>>(c->nelem, NT.feat, NT.params, NT.dS,
-                                                                           part, stride);
+    k_patch_bwd_dB<P><<<NT.nblk_bwd, 256, BwdDims<P>::smem(), c->stream>>>(
+        c->nelem, NT.pt, r, g, NT.Dh, NT.params, NT.gains, NT.dS, part, stride, accumulate);
+    k_mlp_bwd<P><<<NT.nblk_bwd, 256, 0, c->stream>>>(c->nelem, NT.feat, NT.params, NT.dS, part, stride, accumulate);
     k_alpha_part<<<NT.nblk_bwd, 256, 0, c->stream>>>(c->npoin_w, c->lpoin_w, r, g, NT.Dh, NT.params, D::O_ALPHA,
-                                                     part, stride);
+                                                     part, stride, accumulate);
     return 0;
   });
 }
 
-// loss = d^T A d / eAe with d = e - M r; the gradient partials go to part.
-int net_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double eAe, float *part, double *loss) {
+// loss = d^T A d / eAe with d = e - M r; the gradient partials go to part
+// (or are added to it: accumulate).
+int net_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double eAe, float *part, double *loss,
+                  int accumulate = 0) {
   auto &NT = c->net;
   auto &G = c->cg;
   const int nw = c->npoin_w;
@@ -135,7 +130,7 @@ int net_loss_grad(sod_gpu_ctx *c, const double *r, const double *e, double eAe, 
   lap<double>(c, NT.tmp1, NT.tmp2);                                                         // A d
   dots<double, 1>(c, DotArgs<double, 1>{{NT.tmp1}, {NT.tmp2}, {nullptr}}, G.dots + 2);
   k_loss_grad_vec<<<nb, 256, 0, c->stream>>>(nw, c->lpoin_w, NT.tmp2, -2.0 / eAe, NT.tmp2);
-  net_backward(c, r, NT.tmp2, part);
+  net_backward(c, r, NT.tmp2, part, accumulate);
   if (loss) {
     double h;
     CUDA_TRY(cudaMemcpyAsync(&h, G.dots + 2, 8, cudaMemcpyDeviceToHost, c->stream));
@@ -250,10 +245,11 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
   if (!NT.ready) {
     NT.nparam = sod_gpu_precond_num_params(c);
     NT.NP = P == 3 ? NetDims<3>::NP : NetDims<4>::NP;
+    NT.nblk_bwd = 4 * num_sms();  // blocks (and partial rows) of the gradient reductions
     const size_t NPt = (size_t)E * NT.NP;
     if ((rc = c->alloc(&NT.params, NT.nparam)) || (rc = c->alloc(&NT.m1, NT.nparam)) ||
         (rc = c->alloc(&NT.m2, NT.nparam)) || (rc = c->alloc(&NT.grad, NT.nparam)) ||
-        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam * 16)) || (rc = c->alloc(&NT.pt, NPt)) || (rc = c->alloc(&NT.pos, NPt)) ||
+        (rc = c->alloc(&NT.part, (size_t)NT.nblk_bwd * NT.nparam)) || (rc = c->alloc(&NT.pt, NPt)) || (rc = c->alloc(&NT.pos, NPt)) ||
         (rc = c->alloc(&NT.pptr, (size_t)c->npoin + 1)) || (rc = c->alloc(&NT.pslot, NPt)) ||
         (rc = c->alloc(&NT.feat, (size_t)E * NET_F)) || (rc = c->alloc(&NT.gains, (size_t)E * NET_K)) ||
         (rc = c->alloc(&NT.Dh, (size_t)c->npoin)) || (rc = c->alloc(&NT.uf, (size_t)c->npoin)) ||
@@ -263,13 +259,13 @@ int sod_gpu_precond_init(sod_gpu_ctx *c, uint64_t seed, int harvest_capacity) {
     if (P == 3) {
       using D = NetDims<3>;
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
-      CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_dB<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BwdDims<3>::smem()));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)TcDims<3>::smem()));
     } else {
       using D = NetDims<4>;
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::apply_smem(8)));
-      CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_elem<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D::bwd_smem(8)));
+      CUDA_TRY(cudaFuncSetAttribute(k_patch_bwd_dB<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BwdDims<4>::smem()));
       CUDA_TRY(cudaFuncSetAttribute(k_patch_apply_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)TcDims<4>::smem()));
     }
@@ -418,14 +414,14 @@ int sod_gpu_precond_train(sod_gpu_ctx *c, int steps, int batch, float lr, uint64
       k_f2d_w<<<nblk(nw, 256), 256, 0, c->stream>>>(nw, c->lpoin_w, NT.hr + (size_t)k * N, rd);
       k_f2d_w<<<nblk(nw, 256), 256, 0, c->stream>>>(nw, c->lpoin_w, NT.he + (size_t)k * N, ed);
       double l = 0.0;
-      int rc = net_loss_grad(c, rd, ed, NT.eAe[k], NT.part + (size_t)b * NT.nblk_bwd * NT.nparam,
-                             (st == steps - 1) ? &l : nullptr);
+      // the batch's gradient partials add up in one set of block rows
+      int rc = net_loss_grad(c, rd, ed, NT.eAe[k], NT.part, (st == steps - 1) ? &l : nullptr, b > 0);
       if (rc) return rc;
       sum += l;
     }
     NT.step += 1;
     const float bc1 = 1.f - std::pow(0.9f, (float)NT.step), bc2 = 1.f - std::pow(0.999f, (float)NT.step);
-    k_adam<<<nblk(NT.nparam, 256), 256, 0, c->stream>>>(NT.nparam, NT.nblk_bwd * batch, NT.part, NT.params, NT.m1,
+    k_adam<<<nblk(NT.nparam, 256), 256, 0, c->stream>>>(NT.nparam, NT.nblk_bwd, NT.part, NT.params, NT.m1,
                                                         NT.m2, lr, 0.9f, 0.999f, 1e-8f, bc1, bc2, 1.f / batch,
                                                         nullptr);
     NT.gains_ok = false;

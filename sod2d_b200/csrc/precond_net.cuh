@@ -34,7 +34,6 @@ struct NetDims {
   static constexpr size_t apply_smem(int warps) {
     return (size_t)(2 * NPP * NET_K + warps * EPW * (NPP + NET_K)) * 4;
   }
-  static constexpr size_t bwd_smem(int warps) { return (size_t)(NPP * NET_K + warps * EPW * 2 * NPP) * 4; }
 };
 
 __device__ __forceinline__ float softplusf(float a) { return a > 20.f ? a : log1pf(expf(a)); }
@@ -418,25 +417,50 @@ static __global__ void k_patch_gather(long long npoin, const int *__restrict__ p
   z[n] = d * (exp((double)prm[o_alpha]) * d * r[n] + acc);
 }
 
-// Training, per element: x = patch of D^-1/2 r, w = patch of D^-1/2 g
-// (g = dL/dz), h = B x, a = B w; stores X, W (patch rows), Y = s h,
-// SA = s a and dS = h a (dL/ds).
+// Training backward of the patch operator with its B-gradient reduction.
+// Per element: x = patch of D^-1/2 r, w = patch of D^-1/2 g (g = dL/dz),
+// h = B x, a = B w; dS = h a (dL/ds) goes to global memory for the gain
+// MLP, and
+//   dB[k][j] += Y[e][k] W[e][j] + SA[e][k] X[e][j],  Y = s h, SA = s a,
+// is summed in registers: every round the block's 8 warps stage the rows of
+// 4 elements each in shared memory, and each thread adds them to its tile
+// of 4 modes x JB slots, in (warp, element) order.  Block b writes its tile
+// to part[b * stride + O_B + k NP + j], or adds it there (accumulate: the
+// samples of a batch, one launch each, in order; all of it deterministic).
+template <int P>
+struct BwdDims {
+  using D = NetDims<P>;
+  static constexpr int WARPS = 8, JB = (D::NP + 31) / 32;
+  static constexpr int ROW = 2 * D::EPW * D::NPP + 2 * D::EPW * NET_K;  // floats per warp: x, w, Y, SA rows
+  static constexpr size_t smem() { return (size_t)(D::NPP * NET_K + WARPS * ROW) * 4; }
+};
+
 template <int P>
 __global__ void __launch_bounds__(256)
-k_patch_bwd_elem(long long nelem, const int *__restrict__ pt, const double *__restrict__ r,
-                 const double *__restrict__ g, const double *__restrict__ Dh, const float *__restrict__ prm,
-                 const float *__restrict__ gains, float *__restrict__ X, float *__restrict__ W,
-                 float *__restrict__ Y, float *__restrict__ SA, float *__restrict__ dS) {
+k_patch_bwd_dB(long long nelem, const int *__restrict__ pt, const double *__restrict__ r,
+               const double *__restrict__ g, const double *__restrict__ Dh, const float *__restrict__ prm,
+               const float *__restrict__ gains, float *__restrict__ dS, float *__restrict__ part, long long stride,
+               int accumulate) {
   using D = NetDims<P>;
-  constexpr int NPP = D::NPP, K = NET_K, EPW = D::EPW;
+  using Q = BwdDims<P>;
+  constexpr int NPP = D::NPP, NP = D::NP, K = NET_K, EPW = D::EPW, WARPS = Q::WARPS, JB = Q::JB;
+  static_assert(K == 32, "8 blocks of 4 modes");
   extern __shared__ __align__(16) float smem[];
   float *BT = smem;
-  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, nwarps = blockDim.x / 32;
-  float *xs = BT + NPP * K + warp * EPW * 2 * NPP, *ws = xs + EPW * NPP;
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  auto xs_of = [&](int w) { return BT + NPP * K + w * Q::ROW; };
+  float *xs = xs_of(warp), *ws = xs + EPW * NPP, *ys = ws + EPW * NPP, *sas = ys + EPW * K;
   stage_B<P, false>(prm, BT, nullptr);
+  const int k0 = 4 * (threadIdx.x / 32), j0 = JB * (threadIdx.x % 32);
+  float acc[4][JB];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int b = 0; b < JB; ++b) acc[q][b] = 0.f;
   __syncthreads();
-  for (long long gi = (long long)blockIdx.x * nwarps + warp; gi * EPW < nelem; gi += (long long)gridDim.x * nwarps) {
-    const long long e0 = gi * EPW;
+  const long long ngroups = (nelem + EPW - 1) / EPW;
+  for (long long base = (long long)blockIdx.x * WARPS; base < ngroups; base += (long long)gridDim.x * WARPS) {
+    const long long e0 = (base + warp) * EPW;  // past the end: zero rows, no contribution
     gather_patch<P>(e0, nelem, pt, r, Dh, xs, lane);
     gather_patch<P>(e0, nelem, pt, g, Dh, ws, lane);
     __syncwarp();
@@ -446,84 +470,54 @@ k_patch_bwd_elem(long long nelem, const int *__restrict__ pt, const double *__re
 #pragma unroll
     for (int el = 0; el < EPW; ++el) {
       const long long e = e0 + el;
-      if (e >= nelem) continue;
-      const float s = gains[e * K + lane];
-      Y[e * K + lane] = s * h[el];
-      SA[e * K + lane] = s * a[el];
-      dS[e * K + lane] = h[el] * a[el];
-      for (int j = lane; j < D::NP; j += 32) {
-        X[e * D::NP + j] = xs[el * NPP + j];
-        W[e * D::NP + j] = ws[el * NPP + j];
+      const float sg = e < nelem ? gains[e * K + lane] : 0.f;
+      ys[el * K + lane] = sg * h[el];
+      sas[el * K + lane] = sg * a[el];
+      if (e < nelem) dS[e * K + lane] = h[el] * a[el];
+    }
+    __syncthreads();  // the round's rows of every warp are staged
+    for (int w = 0; w < WARPS; ++w) {
+      const float *xw = xs_of(w), *ww = xw + EPW * NPP, *yw = ww + EPW * NPP, *sw = yw + EPW * K;
+#pragma unroll
+      for (int el = 0; el < EPW; ++el) {
+        const float4 y4 = *reinterpret_cast<const float4 *>(yw + el * K + k0);
+        const float4 s4 = *reinterpret_cast<const float4 *>(sw + el * K + k0);
+        const float yv[4] = {y4.x, y4.y, y4.z, y4.w}, sv[4] = {s4.x, s4.y, s4.z, s4.w};
+        float wv[JB], xv[JB];
+#pragma unroll
+        for (int b = 0; b < JB; ++b) {
+          const bool in = j0 + b < NP;
+          wv[b] = in ? ww[el * NPP + j0 + b] : 0.f;
+          xv[b] = in ? xw[el * NPP + j0 + b] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int b = 0; b < JB; ++b) acc[q][b] = fmaf(yv[q], wv[b], fmaf(sv[q], xv[b], acc[q][b]));
       }
     }
-    __syncwarp();
-  }
-}
-
-// dB[k][j] = sum_e Y[e][k] W[e][j] + SA[e][k] X[e][j]; block b sums the
-// contiguous element range [b E / nb, (b+1) E / nb) in element order and
-// writes its partial to part[b * stride + O_B + k NP + j] (deterministic).
-// Each thread owns a tile of 4 modes x JB slots, so an element's row values
-// are loaded once per tile instead of once per entry.
-template <int P>
-__global__ void __launch_bounds__(256)
-k_patch_dB(long long nelem, const float *__restrict__ X, const float *__restrict__ W, const float *__restrict__ Y,
-           const float *__restrict__ SA, float *__restrict__ part, long long stride) {
-  using D = NetDims<P>;
-  constexpr int NP = D::NP, K = NET_K, CH = 8, JB = (NP + 31) / 32, NPJ = 32 * JB;
-  static_assert(K == 32, "8 blocks of 4 modes");
-  __shared__ __align__(16) float Xs[CH][NPJ], Ws[CH][NPJ], Ys[CH][K], Ss[CH][K];
-  const long long lo = nelem * blockIdx.x / gridDim.x, hi = nelem * (blockIdx.x + 1) / gridDim.x;
-  const int k0 = 4 * (threadIdx.x / 32), j0 = JB * (threadIdx.x % 32);
-  float acc[4][JB];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < JB; ++b) acc[a][b] = 0.f;
-  for (long long c0 = lo; c0 < hi; c0 += CH) {
-    const int nc = (int)((hi - c0) < CH ? (hi - c0) : CH);
-    __syncthreads();
-    for (int i = threadIdx.x; i < nc * NPJ; i += blockDim.x) {
-      const int el = i / NPJ, j = i % NPJ;
-      Xs[el][j] = j < NP ? X[(c0 + el) * NP + j] : 0.f;
-      Ws[el][j] = j < NP ? W[(c0 + el) * NP + j] : 0.f;
-    }
-    for (int i = threadIdx.x; i < nc * K; i += blockDim.x) {
-      const int el = i / K, k = i % K;
-      Ys[el][k] = Y[(c0 + el) * K + k];
-      Ss[el][k] = SA[(c0 + el) * K + k];
-    }
-    __syncthreads();
-    for (int el = 0; el < nc; ++el) {
-      const float4 y4 = *reinterpret_cast<const float4 *>(&Ys[el][k0]);
-      const float4 s4 = *reinterpret_cast<const float4 *>(&Ss[el][k0]);
-      const float yv[4] = {y4.x, y4.y, y4.z, y4.w}, sv[4] = {s4.x, s4.y, s4.z, s4.w};
-      float wv[JB], xv[JB];
-#pragma unroll
-      for (int b = 0; b < JB; ++b) { wv[b] = Ws[el][j0 + b]; xv[b] = Xs[el][j0 + b]; }
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < JB; ++b) acc[a][b] = fmaf(yv[a], wv[b], fmaf(sv[a], xv[b], acc[a][b]));
-    }
+    __syncthreads();  // the rows are rewritten by the next round
   }
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
+  for (int q = 0; q < 4; ++q)
 #pragma unroll
     for (int b = 0; b < JB; ++b)
-      if (j0 + b < NP) part[blockIdx.x * stride + D::O_B + (k0 + a) * NP + j0 + b] = acc[a][b];
+      if (j0 + b < NP) {
+        float *o = part + blockIdx.x * stride + D::O_B + (k0 + q) * NP + j0 + b;
+        *o = (accumulate ? *o : 0.f) + acc[q][b];
+      }
 }
 
-// Gradient of the gain MLP from dS = dL/ds; block b covers the same element
-// range as k_patch_dB.  The weights are staged in shared memory (W2 and W3
-// also transposed, so the backward matrix-vector products read rows lane by
-// lane); each lane accumulates its column of every weight gradient in
-// registers over its warp's elements, and the block adds the warps'
-// gradients in warp order into part (deterministic).
+// Gradient of the gain MLP from dS = dL/ds; block b covers the contiguous
+// element range [b E / nb, (b+1) E / nb).  The weights are staged in shared
+// memory (W2 and W3 also transposed, so the backward matrix-vector products
+// read rows lane by lane); each lane accumulates its column of every weight
+// gradient in registers over its warp's elements, and the block adds the
+// warps' gradients in warp order into part, or onto it (accumulate).
 template <int P>
 __global__ void __launch_bounds__(256)
 k_mlp_bwd(long long nelem, const float *__restrict__ feat, const float *__restrict__ prm,
-          const float *__restrict__ dS, float *__restrict__ part, long long stride) {
+          const float *__restrict__ dS, float *__restrict__ part, long long stride, int accumulate) {
   using D = NetDims<P>;
   constexpr int H = NET_H, K = NET_K, F = NET_F, NM = D::NMLP;
   static_assert(H == 32 && K == 32, "one lane per hidden unit and per mode");
@@ -605,14 +599,18 @@ k_mlp_bwd(long long nelem, const float *__restrict__ feat, const float *__restri
     }
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < NM; i += blockDim.x) part[blockIdx.x * stride + D::O_W1T + i] = acc[i];
+  for (int i = threadIdx.x; i < NM; i += blockDim.x) {
+    float *o = part + blockIdx.x * stride + D::O_W1T + i;
+    *o = (accumulate ? *o : 0.f) + acc[i];
+  }
 }
 
 // dL/dalpha partial: exp(alpha) sum over the block's working nodes of
 // (D^-1/2 g)(D^-1/2 r), written to part[b * stride + o_alpha].
 static __global__ void k_alpha_part(int npoin_w, const int *__restrict__ lpoin_w, const double *__restrict__ r,
                              const double *__restrict__ g, const double *__restrict__ Dh,
-                             const float *__restrict__ prm, int o_alpha, float *__restrict__ part, long long stride) {
+                             const float *__restrict__ prm, int o_alpha, float *__restrict__ part, long long stride,
+                             int accumulate) {
   __shared__ double sh[256];
   const long long lo = (long long)npoin_w * blockIdx.x / gridDim.x,
                   hi = (long long)npoin_w * (blockIdx.x + 1) / gridDim.x;
@@ -627,7 +625,10 @@ static __global__ void k_alpha_part(int npoin_w, const int *__restrict__ lpoin_w
     if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[blockIdx.x * stride + o_alpha] = (float)(exp((double)prm[o_alpha]) * sh[0]);
+  if (threadIdx.x == 0) {
+    float *o = part + blockIdx.x * stride + o_alpha;
+    *o = (accumulate ? *o : 0.f) + (float)(exp((double)prm[o_alpha]) * sh[0]);
+  }
 }
 
 // grad[i] = sum over blocks of part[b][i] (fixed order), then Adam.
