@@ -42,8 +42,8 @@ sys.path.insert(0, str(ROOT))
 B_PER_NODE_STAGE = 402.0
 # DRAM bytes (read + write) of one RHS evaluation per working node, from one
 # ncu capture of the four RHS kernels on the 64^3 workload itself
-# (5,558,146,304 B for 7,077,888 working nodes).
-DRAM_B_PER_NODE_STAGE = 5558146304 / 7077888
+# (5,578,256,128 B for 7,077,888 working nodes).
+DRAM_B_PER_NODE_STAGE = 5578256128 / 7077888
 NELEM_1D = 64
 PORDER = 3
 
@@ -385,8 +385,6 @@ def imex_step_leg(nelem1d=NELEM_1D, stages=4, steps=10, warmup=3, Ma=1.25, cfl=0
     import ctypes as C
     import torch
     from sod2d_b200 import gpu, host
-    if dt is None:  # 0.01 on the 32^3 mesh, the same convective CFL on finer meshes
-        dt = 0.01 * 32 / nelem1d
     m = host.periodic_cube(PORDER, nelem1d)
     ic = host.tgv_comp_init(m, Ma=Ma)
     sv = gpu.CompSolver(m, ic, stages=stages, fp64_state=False, cfl_conv=cfl, cfl_diff=1000.5, imex=True)

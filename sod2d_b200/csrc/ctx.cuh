@@ -313,15 +313,23 @@ inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
 template <int P>
 struct Launch {
   static constexpr int P_ = P;
-  static constexpr int EPB = (Cfg<P>::NT <= 64) ? 2 : 1;
+  // One element per block (64 threads for P=3, 128 for P=4) for every
+  // element kernel but pass A, whose latency-bound gathers do better with
+  // two elements per block for P=3 (0.405 against 0.447 ms at 64^3), while
+  // pass B and the Laplacian do better with one (0.94 against 1.05 ms).
+  static constexpr int EPB = 1;
   static constexpr int TPB = EPB * Cfg<P>::NT;
+  static constexpr int EPB_A = (Cfg<P>::NT <= 64) ? 2 : 1;
+  static constexpr int TPB_A = EPB_A * Cfg<P>::NT;
   static unsigned grid(int nelem) { return nblk(nelem, EPB); }
 
   static void proj(sod_gpu_ctx *c, bool prim, const float *a0, const float *a1, const float *a2) {
     if (prim)
-      k_proj<P, EPB, true><<<grid(c->nelem), TPB, 0, c->stream>>>(c->md(), c->ph, c->phys.Rgas, a0, a1, a2, c->slotsA);
+      k_proj<P, EPB_A, true><<<nblk(c->nelem, EPB_A), TPB_A, 0, c->stream>>>(c->md(), c->ph, c->phys.Rgas, a0, a1, a2,
+                                                                          c->slotsA);
     else
-      k_proj<P, EPB, false><<<grid(c->nelem), TPB, 0, c->stream>>>(c->md(), c->ph, c->phys.Rgas, a0, a1, a2, c->slotsA);
+      k_proj<P, EPB_A, false><<<nblk(c->nelem, EPB_A), TPB_A, 0, c->stream>>>(c->md(), c->ph, c->phys.Rgas, a0, a1,
+                                                                           a2, c->slotsA);
   }
   // Persistent pass B: as many blocks as fit on the GPU at once (at most
   // one per element group), each walking the groups with a stride.

@@ -19,9 +19,8 @@
 #ifndef SOD_VEC_XI
 #define SOD_VEC_XI 1
 #endif
-#ifndef SOD_RHS_MINB
-#define SOD_RHS_MINB 4
-#endif
+// Pass-B blocks resident per SM: 512 threads per SM, 128 registers each.
+#define SOD_RHS_THREADS_PER_SM 512
 
 namespace sod {
 
@@ -299,7 +298,7 @@ struct RhsPlan {
 // blockIdx.x, blockIdx.x + gridDim.x, ... and, while it computes one group,
 // its cp.async copies bring the next group's inputs into the other stage.
 template <int P, int EPB, int MODE, int IN>
-__global__ void __launch_bounds__(EPB *Cfg<P>::NT, SOD_RHS_MINB)
+__global__ void __launch_bounds__(EPB *Cfg<P>::NT, SOD_RHS_THREADS_PER_SM / (EPB * Cfg<P>::NT))
 k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   using L = RhsPlan<P, EPB, MODE, IN>;
   constexpr int N1 = L::N1, N = L::N, NT = L::NT, NTB = L::NTB, NC = L::NC, SMF = L::SMF, PB_T = L::PB_T;
