@@ -56,6 +56,7 @@ struct sod_gpu_ctx {
   // scratch
   float *slotsA = nullptr, *slotsB = nullptr, *proj12 = nullptr, *mue_t = nullptr, *musgs_t = nullptr;
   unsigned *vbits = nullptr;  // minimum density of the standalone smart_visc_spectral_imex
+  int *err_h = nullptr, *err_d = nullptr;  // mapped pinned flag (host / device view) of a device wait that gave up
   size_t bytes = 0;
   std::vector<void *> allocs;
   std::vector<void *> host_allocs;  // pinned host memory
@@ -183,7 +184,19 @@ struct sod_gpu_ctx {
   }
   int finish() {
     CUDA_TRY(cudaGetLastError());
-    if (!async) CUDA_TRY(cudaStreamSynchronize(stream));
+    if (!async) {
+      CUDA_TRY(cudaStreamSynchronize(stream));
+      return check_waits();
+    }
+    return 0;
+  }
+  // A bounded wait inside a kernel that gave up (a bulk copy that never
+  // completed) is reported once, at the next synchronisation.
+  int check_waits() {
+    if (err_h && *(volatile int *)err_h) {
+      *(volatile int *)err_h = 0;
+      return fail(SOD_GPU_ECUDA, "a bulk copy into shared memory did not complete");
+    }
     return 0;
   }
 };
@@ -345,7 +358,9 @@ struct Launch {
     }();
     const long long groups = grid(c->nelem);
     const unsigned g = (unsigned)std::min<long long>(groups, (long long)per_sm * num_sms());
-    k_rhs<P, EPB, MODE, IN><<<g, TPB, PL::BYTES, c->stream>>>(c->md(), c->ph, c->phys.Rgas, A, c->slotsB);
+    RhsArgs Ae = A;
+    Ae.err = c->err_d;
+    k_rhs<P, EPB, MODE, IN><<<g, TPB, PL::BYTES, c->stream>>>(c->md(), c->ph, c->phys.Rgas, Ae, c->slotsB);
   }
 };
 

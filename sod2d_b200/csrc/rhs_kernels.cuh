@@ -142,6 +142,42 @@ __device__ __forceinline__ void cp_async16(float *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Bulk (TMA) copies of contiguous per-element data into shared memory,
+// completed on an mbarrier (transaction count).
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// dst (shared) and src (global) 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// Bounded wait for the phase `parity` of bar (try_wait itself suspends the
+// thread for a while): false after SOD_BULK_WAIT_LIMIT polls.
+#ifndef SOD_BULK_WAIT_LIMIT
+#define SOD_BULK_WAIT_LIMIT (1 << 24)
+#endif
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  for (int it = 0; it < SOD_BULK_WAIT_LIMIT; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
 // ---------------------------------------------------------------------
 // Pass A: LPS projections (full_proj_ijk, elem_stab.f90:474-562).  Writes
 // gpvol * {tau00, tau01, tau02, tau11, tau12, tau22, grad rho (3), grad T
@@ -256,6 +292,7 @@ struct RhsArgs {
   const float *proj12;    // [npoin][12] mass-inverted projections (internal):
                           // tau00 tau01 tau02 tau11 tau12 tau22 gradRho(3) gradT(3)
   float fact_c, fact_d;
+  int *err;  // mapped host flag: set when a bulk-copy wait of pass B gave up
 };
 
 // Staged pairs of pass B, one float2 per element node:
@@ -311,6 +348,20 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   float *const sf = dsm + L::O_STG + el * SMF * N;
   float2 *const sp = reinterpret_cast<float2 *>(sf);
   const float invR = __frcp_rn(Rgas);
+  // P = 3, one element per block: the element's J^-1 and gpvol (2560 B),
+  // slot positions and mu_e (256 B each) are contiguous and 16-byte aligned
+  // in global memory, and land with the stage's layout (stride N = NTB), so
+  // one thread moves them with bulk copies; the gathered state and
+  // projections stay per-thread cp.async.
+  constexpr bool BULK = (P == 3 && EPB == 1);
+  __shared__ __align__(8) unsigned long long mbar[2];
+  unsigned phases = 0u;  // bit b: parity of the next completion of mbar[b]
+  if (BULK && tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (BULK) __syncthreads();
 
   auto node_of = [&](long long g) -> int {
     const long long e = g * EPB + el;
@@ -318,6 +369,18 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
   };
   // this thread's copies for group g into stage stg (nd: its node, -1: none)
   auto issue = [&](float *stg, long long g, int nd) {
+    if (BULK && tid == 0 && g < ngroups) {
+      const long long e0 = g;  // one element per block
+      unsigned long long *bar = &mbar[stg == dsm ? 0 : 1];
+      const bool mus = DIFF && A.musgs_t;
+      const unsigned bytes = (10u + 1u + (DIFF ? 1u : 0u) + (mus ? 1u : 0u)) * N * 4u;
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // earlier reads of this stage first
+      mbar_expect_tx(bar, bytes);
+      bulk_g2s(stg + L::O_GEO, m.geo + e0 * 10 * N, 10u * N * 4u, bar);
+      bulk_g2s(stg + L::O_POS, m.slot_pos + e0 * N, N * 4u, bar);
+      if (DIFF) bulk_g2s(stg + L::O_MUE, A.mue_t + e0 * N, N * 4u, bar);
+      if (mus) bulk_g2s(stg + L::O_MUS, A.musgs_t + e0 * N, N * 4u, bar);
+    }
     if (nd < 0) return;
     const long long e = g * EPB + el;
     if (IN == IN_CONS) {
@@ -343,13 +406,17 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
       cp_async4(stg + L::O_IN + 5 * NTB + tid, A.Tem + nd);
       cp_async4(stg + L::O_IN + 6 * NTB + tid, A.mu_fluid + nd);
     }
-    const float *g0 = m.geo + e * 10 * N + t;
+    if (!BULK) {
+      const float *g0 = m.geo + e * 10 * N + t;
 #pragma unroll
-    for (int c = 0; c < 10; ++c) cp_async4(stg + L::O_GEO + c * NTB + tid, g0 + c * N);
-    cp_async4(stg + L::O_POS + tid, m.slot_pos + e * N + t);
+      for (int c = 0; c < 10; ++c) cp_async4(stg + L::O_GEO + c * NTB + tid, g0 + c * N);
+      cp_async4(stg + L::O_POS + tid, m.slot_pos + e * N + t);
+    }
     if (DIFF) {
-      cp_async4(stg + L::O_MUE + tid, A.mue_t + e * N + t);
-      if (A.musgs_t) cp_async4(stg + L::O_MUS + tid, A.musgs_t + e * N + t);
+      if (!BULK) {
+        cp_async4(stg + L::O_MUE + tid, A.mue_t + e * N + t);
+        if (A.musgs_t) cp_async4(stg + L::O_MUS + tid, A.musgs_t + e * N + t);
+      }
       if (LPS) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) cp_async16(stg + L::O_PROJ + tid * 12 + 4 * c, A.proj12 + (long long)nd * 12 + 4 * c);
@@ -365,6 +432,11 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
     const float *cur = dsm + buf * L::STAGE;
     float *nxt = dsm + (buf ^ 1) * L::STAGE;
     cp_async_wait_all();  // this thread's copies of the current group have landed
+    bool bulk_ok = true;
+    if (BULK) {  // and the block's bulk copies of it
+      bulk_ok = mbar_wait(&mbar[buf], (phases >> buf) & 1u);
+      phases ^= 1u << buf;
+    }
     const long long e = g * EPB + el;
     const bool active = (e < m.nelem) && (t < N);
     const float *gm = cur + L::O_GEO + tid;  // J^-1 (9 components) and gpvol, stride NTB
@@ -405,7 +477,11 @@ k_rhs(MeshDev m, Phys ph, float Rgas, RhsArgs A, float *__restrict__ slots) {
       }
       if (DIFF) sp[PB_T * N + t] = make_float2(s.T, 0.f);
     }
-    __syncthreads();  // staged pairs visible; every thread is done with the other stage
+    // staged pairs visible; every thread is done with the other stage
+    if (!__syncthreads_and(bulk_ok)) {
+      if (tid == 0) *(volatile int *)A.err = 1;  // a bulk copy never completed: stop, nothing else is in flight
+      return;
+    }
     if (g + G < ngroups) issue(nxt, g + G, nd_next);
     cp_async_commit();
     nd_next = node_of(g + 2 * G);  // consumed one group later

@@ -103,6 +103,20 @@ int sod_gpu_init(const sod_mesh_t *mesh, const sod_phys_t *phys, sod_gpu_ctx **o
     sod_gpu_finalize(c);
     return rc;
   }
+  {
+    void *h = nullptr;
+    if (cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped) != cudaSuccess) {
+      sod_gpu_finalize(c);
+      return fail(SOD_GPU_ENOMEM, "cudaHostAlloc of the wait flag failed");
+    }
+    c->host_allocs.push_back(h);
+    c->err_h = (int *)h;
+    *c->err_h = 0;
+    if (cudaHostGetDevicePointer((void **)&c->err_d, h, 0) != cudaSuccess) {
+      sod_gpu_finalize(c);
+      return fail(SOD_GPU_ECUDA, "cudaHostGetDevicePointer of the wait flag failed");
+    }
+  }
   if ((rc = c->alloc(&c->cg.dticket, 1)) || (rc = c->alloc(&c->cg.part, (size_t)8 * DOT_BLOCKS)) ||
       (rc = c->alloc(&c->cg.dots, 16))) {
     sod_gpu_finalize(c);
@@ -164,7 +178,7 @@ int sod_gpu_set_async(sod_gpu_ctx *ctx, int enabled) {
 int sod_gpu_synchronize(sod_gpu_ctx *ctx) {
   if (!ctx) return fail(SOD_GPU_EINVAL, "null context");
   CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-  return 0;
+  return ctx->check_waits();
 }
 
 int sod_gpu_set_halo(sod_gpu_ctx *c, int rank, int nnb, const int *ranksToComm, const int *commsMemPosInLoc,
