@@ -20,7 +20,9 @@
 #define SOD_VEC_XI 1
 #endif
 // Pass-B blocks resident per SM: 512 threads per SM, 128 registers each.
+#ifndef SOD_RHS_THREADS_PER_SM
 #define SOD_RHS_THREADS_PER_SM 512
+#endif
 
 namespace sod {
 
