@@ -1,7 +1,7 @@
 """bench.py end to end on a small mesh: every leg of the default JSON line
 (RHS, end-to-end copies, RK and IMEX time steps, the pressure-solve
-comparison, the CPU baseline) runs and the line carries the contract's
-keys.  The legs are those of the default run, at sizes that take seconds."""
+comparison, the CPU baseline) runs, and the line carries every key of the
+bench line format.  The legs are those of the default run, at sizes that take seconds."""
 import json
 import subprocess
 import sys
