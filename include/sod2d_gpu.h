@@ -18,7 +18,10 @@
  *  - All calls are complete on return (the reference's OpenACC regions are
  *    synchronous), unless sod_gpu_set_stream() selected a stream and
  *    sod_gpu_set_async(ctx, 1) was called, in which case work is only
- *    enqueued on that stream.
+ *    enqueued on that stream.  Kernels that wait on their own bulk copies
+ *    bound every wait; a wait that gave up (never expected) is reported as
+ *    SOD_GPU_ECUDA by the next call that synchronises (every call when not
+ *    asynchronous, sod_gpu_synchronize() otherwise).
  *  - Functions return 0 on success and a negative SOD_GPU_E* code on error;
  *    sod_gpu_last_error() describes the last failure of the calling thread.
  *    The Fortran shim turns a non-zero status into `stop 1`.
