@@ -42,8 +42,8 @@ sys.path.insert(0, str(ROOT))
 B_PER_NODE_STAGE = 402.0
 # DRAM bytes (read + write) of one RHS evaluation per working node, from one
 # ncu capture of the four RHS kernels on the 64^3 workload itself
-# (5,578,256,128 B for 7,077,888 working nodes).
-DRAM_B_PER_NODE_STAGE = 5578256128 / 7077888
+# (5,535,995,392 B for 7,077,888 working nodes).
+DRAM_B_PER_NODE_STAGE = 5535995392 / 7077888
 NELEM_1D = 64
 PORDER = 3
 
