@@ -190,8 +190,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned pari
 // Input: conserved state (SoA, reference layout) -> EOS in registers, or
 // primitive rho/u/T (prim = true).
 // ---------------------------------------------------------------------
+// P = 3: 16 blocks per SM (32 registers, full occupancy) hide more of the
+// latency of the state gather: 1.636 against 1.643 ms per RHS at 64^3 with
+// 44 registers (11 blocks); 40 registers (12 blocks) gave 1.643.
 template <int P, int EPB, bool PRIM>
-__global__ void __launch_bounds__(EPB *Cfg<P>::NT)
+__global__ void __launch_bounds__(EPB *Cfg<P>::NT, P == 3 ? 16 : 1)
 k_proj(MeshDev m, Phys ph, float Rgas, const float *__restrict__ a0, const float *__restrict__ a1,
        const float *__restrict__ a2, float *__restrict__ slots) {
   constexpr int N1 = Cfg<P>::N1, N = Cfg<P>::N, NT = Cfg<P>::NT, NF = 5;
